@@ -1,0 +1,117 @@
+"""ctypes binding of the in-tree CUDA library ``libbmm_b200.so``.
+
+There is no CPU fallback: if the library is missing, every call raises.  Status
+codes map to the exception classes the reference's bindings raise for the
+corresponding C++ exceptions (std::invalid_argument -> ValueError,
+std::overflow_error -> OverflowError, std::runtime_error -> RuntimeError).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbmm_b200.so")
+
+OK, EINVAL, EOVERFLOW, ECUDA, ENODEV, ETIMEOUT, ENOMEM = 0, -1, -2, -3, -4, -5, -6
+
+
+class Candidate_t(C.Structure):
+    _fields_ = [("mask", C.c_uint64), ("weight", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Features_t(C.Structure):
+    _fields_ = [("cuda_compiled", C.c_int), ("cuda_available", C.c_int),
+                ("device_count", C.c_int), ("sm_count", C.c_int), ("cc_major", C.c_int),
+                ("cc_minor", C.c_int), ("device_name", C.c_char * 64)]
+
+
+CAND_DTYPE = np.dtype([("mask", np.uint64), ("weight", np.uint32), ("reserved", np.uint32)])
+
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_i16p = C.POINTER(C.c_int16)
+_sz = C.c_size_t
+_szp = C.POINTER(C.c_size_t)
+_vp = C.c_void_p
+_candp = C.POINTER(Candidate_t)
+
+# name -> argtypes (all return int unless listed in _RESTYPES)
+SIGNATURES = {
+    "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
+    "bmm_last_error": [],
+    "bmm_version": [],
+    "bmm_runtime_features": [C.POINTER(Features_t)],
+    "bmm_fwht_i32": [_i32p, _sz],
+    "bmm_fwht_i16": [_i16p, _sz],
+    "bmm_fwht_i32_dev": [_vp, _sz, _vp],
+    "bmm_fwht_search": [_u64p, _sz, _sz, _u32p, _sz, _sz, _sz, _candp, _szp],
+    "bmm_gray_search": [_u64p, _sz, _sz, _u32p, _sz, _sz, _sz, _candp, _szp],
+    "bmm_gray_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, C.c_int, _u64p, _u32p],
+    "bmm_gray_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, C.c_int, _vp, _vp, _vp],
+    "bmm_fwht_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, _u64p, _u32p],
+    "bmm_fwht_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp, _vp],
+}
+_RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
+             "bmm_gen_instance": C.c_uint64}
+
+_lib = None
+
+
+def lib():
+    """Load libbmm_b200.so (raises ImportError when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m bmmpy_b200.build`; "
+                "bmmpy_b200 has no CPU fallback")
+        L = C.CDLL(LIB_PATH)
+        for name, args in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = _RESTYPES.get(name, C.c_int)
+        _lib = L
+    return _lib
+
+
+def has(name: str) -> bool:
+    return hasattr(lib(), name)
+
+
+def last_error() -> str:
+    msg = lib().bmm_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(rc: int, what: str = "") -> None:
+    if rc == OK:
+        return
+    msg = last_error() or what
+    if rc == EINVAL:
+        raise ValueError(msg)
+    if rc == EOVERFLOW:
+        raise OverflowError(msg)
+    if rc == ENOMEM:
+        raise MemoryError(msg)
+    raise RuntimeError(f"{msg} (status {rc})")
+
+
+def ptr(a: np.ndarray, typ):
+    return a.ctypes.data_as(typ)
+
+
+def u64p(a):
+    return ptr(a, _u64p)
+
+
+def u32p(a):
+    return ptr(a, _u32p)
+
+
+def candp(a):
+    return a.ctypes.data_as(_candp)

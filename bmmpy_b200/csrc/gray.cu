@@ -1,0 +1,380 @@
+// Gray-code exhaustive search on sm_100a.
+//
+// Reference behaviour: BruteforceSearch::search / sweep_prefix
+// (src/search/bruteforce_search.cpp:126-170,300-329) and the CUDA twin
+// bruteforce_persistent_kernel (src/search/cuda_bruteforce_launch.cu:131-296):
+// split the t-bit mask into a high prefix and a low chunk, start each prefix
+// from the XOR of its high rows, then walk the 2^chunk low states in
+// reflected-Gray order (one row XOR + full popcount per step).
+//
+// B200 design (not the reference's): one LANE owns one prefix and keeps the
+// whole current row (WPL words) in registers, so a step is WPL XOR+POPC with
+// no shuffle; every lane of a warp flips the same row at the same step, so
+// the row words come from shared memory as broadcast 128-bit loads.  Rows
+// wider than 64 words are split over G lanes (words [g*WPL, (g+1)*WPL) in
+// lane g of the group) with a log2(G) shuffle reduction per step.  Top-k
+// lives in the warp's registers (WarpTopK); top-1 per target is a register
+// min folded with one 64-bit atomicMin per warp.
+#include "common.cuh"
+#include "gray.cuh"
+#include "topk.cuh"
+
+namespace bmm {
+namespace {
+
+constexpr int kThreads = 128;
+
+template <int WPL>
+__device__ __forceinline__ uint32_t xor_row_popc(uint64_t (&cur)[WPL], const uint64_t* srow) {
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(srow);
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < WPL / 2; ++i) {
+        const ulonglong2 v = p[i];
+        cur[2 * i] ^= v.x;
+        cur[2 * i + 1] ^= v.y;
+        s += __popcll(cur[2 * i]) + __popcll(cur[2 * i + 1]);
+    }
+    return s;
+}
+
+template <int WPL>
+__device__ __forceinline__ void xor_row(uint64_t (&cur)[WPL], const uint64_t* srow) {
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(srow);
+#pragma unroll
+    for (int i = 0; i < WPL / 2; ++i) {
+        const ulonglong2 v = p[i];
+        cur[2 * i] ^= v.x;
+        cur[2 * i + 1] ^= v.y;
+    }
+}
+
+template <int WPL>
+__device__ __forceinline__ uint32_t popc_row(const uint64_t (&cur)[WPL]) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = 0; i < WPL; ++i)
+        s += __popcll(cur[i]);
+    return s;
+}
+
+template <int G>
+__device__ __forceinline__ uint32_t group_sum(uint32_t v) {
+#pragma unroll
+    for (int o = 1; o < G; o <<= 1)
+        v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// Stage `nrows` rows (row r from src + idx(r) * stride, W words) into shared
+// memory as nrows x (G*WPL) words, zero padded.
+template <int WPL, int G, typename RowOf>
+__device__ __forceinline__ void stage_rows(uint64_t* srow, int nrows, int W, RowOf row_of) {
+    constexpr int SW = WPL * G;
+    for (int i = threadIdx.x; i < nrows * SW; i += blockDim.x) {
+        const int r = i / SW, w = i % SW;
+        srow[i] = w < W ? row_of(r)[w] : 0ull;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Window search: top-kk over all nonzero masks of t rows.
+// rows: t x W words (device, packed in window order).
+template <int WPL, int G, int E>
+__global__ void __launch_bounds__(kThreads)
+    gray_window_kernel(const uint64_t* __restrict__ rows, int t, int W, int chunk,
+                       unsigned long long n_prefix, int kk, bmm_candidate* __restrict__ cta_out) {
+    extern __shared__ __align__(16) uint64_t srow[];
+    constexpr int SW = WPL * G;
+    stage_rows<WPL, G>(srow, t, W, [&](int r) { return rows + (size_t)r * W; });
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;  // lane within the group
+    const unsigned long long groups_per_cta = kThreads / G;
+    const unsigned long long stride_groups = groups_per_cta * gridDim.x;
+    unsigned long long p = blockIdx.x * groups_per_cta + threadIdx.x / G;
+    const int hb = t - chunk;
+    const uint32_t states = 1u << chunk;
+
+    WarpTopK<E> top;
+    top.init();
+    uint32_t thr = 0xffffffffu;
+
+    const uint64_t* my = srow + gl * WPL;
+    while (__any_sync(kFull, p < n_prefix)) {
+        const bool valid = p < n_prefix && gl == 0;
+        uint64_t cur[WPL];
+#pragma unroll
+        for (int i = 0; i < WPL; ++i)
+            cur[i] = 0;
+        for (int b = 0; b < hb; ++b)
+            if ((p >> b) & 1ull)
+                xor_row<WPL>(cur, my + (size_t)(chunk + b) * SW);
+        uint64_t mask = (uint64_t)p << chunk;
+        uint32_t w = group_sum<G>(popc_row<WPL>(cur));
+        top.offer(valid && mask != 0, w, mask, kk, thr);
+        for (uint32_t s = 1; s < states; ++s) {
+            const int b = __ffs(s) - 1;
+            w = group_sum<G>(xor_row_popc<WPL>(cur, my + (size_t)b * SW));
+            mask ^= 1ull << b;
+            top.offer(valid, w, mask, kk, thr);
+        }
+        p += stride_groups;
+    }
+
+    // merge the CTA's warps: warps 1.. offer their lists to warp 0 via smem
+    __syncthreads();
+    bmm_candidate* stage = reinterpret_cast<bmm_candidate*>(srow);
+    const int warp = threadIdx.x >> 5;
+    top.store(stage + warp * 32 * E, 32 * E);
+    __syncthreads();
+    if (warp == 0) {
+        for (int ow = 1; ow < kThreads / 32; ++ow) {
+            for (int base = 0; base < 32 * E; base += 32) {
+                const bmm_candidate c = stage[ow * 32 * E + base + lane];
+                const bool ok = c.weight != 0xffffffffu;
+                if (!__any_sync(kFull, ok && c.weight <= thr))
+                    break;  // lists are sorted: nothing further can enter
+                top.offer(ok, c.weight, c.mask, kk, thr);
+            }
+        }
+        top.store(cta_out + (size_t)blockIdx.x * kk, kk);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-target top-1.  CTA b serves target b / ctas_per_target.
+// key = (weight << 40) | tie, tie = S (tiebreak 0) or inverse-Gray(S).
+template <int WPL, int G>
+__global__ void __launch_bounds__(kThreads)
+    gray_targets_kernel(const uint64_t* __restrict__ words, int stride, int W,
+                        const uint32_t* __restrict__ targets, const uint32_t* __restrict__ others,
+                        int k, int chunk, int tiebreak, int ctas_per_target,
+                        unsigned long long* __restrict__ best_keys) {
+    extern __shared__ __align__(16) uint64_t srow[];
+    constexpr int SW = WPL * G;
+    const int ti = blockIdx.x / ctas_per_target;
+    const int part = blockIdx.x % ctas_per_target;
+    const uint32_t* oth = others + (size_t)ti * k;
+    const uint32_t tgt = targets[ti];
+    // rows 0..k-1: others, row k: the target
+    stage_rows<WPL, G>(srow, k + 1, W, [&](int r) {
+        return words + (size_t)(r < k ? oth[r] : tgt) * stride;
+    });
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int gl = lane % G;
+    const int hb = k - chunk;
+    const unsigned long long n_prefix = 1ull << hb;
+    const unsigned long long p = (unsigned long long)part * (kThreads / G) + threadIdx.x / G;
+    const bool valid = p < n_prefix && gl == 0;
+    const uint64_t* my = srow + gl * WPL;
+
+    uint64_t cur[WPL];
+    {
+        const ulonglong2* tp = reinterpret_cast<const ulonglong2*>(my + (size_t)k * SW);
+#pragma unroll
+        for (int i = 0; i < WPL / 2; ++i) {
+            const ulonglong2 v = tp[i];
+            cur[2 * i] = v.x;
+            cur[2 * i + 1] = v.y;
+        }
+    }
+    for (int b = 0; b < hb; ++b)
+        if ((p >> b) & 1ull)
+            xor_row<WPL>(cur, my + (size_t)(chunk + b) * SW);
+
+    const uint64_t lowmask = (1ull << chunk) - 1;
+    const uint64_t hi_mask = p << chunk;
+    // tie key for the Gray order: inverse-Gray(S) = (ig(p) << chunk) | (s ^ flip)
+    const uint64_t hi_tie = tiebreak ? (inverse_gray64(p) << chunk) : hi_mask;
+    const uint64_t flip = (tiebreak && (__popcll(p) & 1)) ? lowmask : 0ull;
+
+    uint32_t best_w = group_sum<G>(popc_row<WPL>(cur));
+    uint64_t best_tie = tiebreak ? (hi_tie | flip) : hi_mask;
+    uint64_t low = 0;
+    const uint32_t states = 1u << chunk;
+    for (uint32_t s = 1; s < states; ++s) {
+        const int b = __ffs(s) - 1;
+        const uint32_t w = group_sum<G>(xor_row_popc<WPL>(cur, my + (size_t)b * SW));
+        low ^= 1ull << b;
+        if (w <= best_w) {
+            const uint64_t tie = tiebreak ? (hi_tie | (s ^ flip)) : (hi_mask | low);
+            if (w < best_w || tie < best_tie) {
+                best_w = w;
+                best_tie = tie;
+            }
+        }
+    }
+    unsigned long long key = valid ? (((unsigned long long)best_w << 40) | best_tie) : ~0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(kFull, key, o);
+        key = other < key ? other : key;
+    }
+    if (lane == 0 && key != ~0ull)
+        atomicMin(best_keys + ti, key);
+}
+
+// Decode keys into (mask, weight).
+__global__ void decode_keys_kernel(const unsigned long long* __restrict__ keys, int n, int tiebreak,
+                                   uint64_t* __restrict__ best_mask,
+                                   uint32_t* __restrict__ best_weight) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const unsigned long long key = keys[i];
+    const uint64_t tie = key & ((1ull << 40) - 1);
+    // S = gray(tie) when the tie key is the Gray index
+    best_mask[i] = tiebreak ? (tie ^ (tie >> 1)) : tie;
+    best_weight[i] = (uint32_t)(key >> 40);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+int group_shape(size_t W, int* wpl, int* g) {
+    if (W <= 2) {
+        *wpl = 2, *g = 1;
+    } else if (W <= 4) {
+        *wpl = 4, *g = 1;
+    } else if (W <= 8) {
+        *wpl = 8, *g = 1;
+    } else if (W <= 16) {
+        *wpl = 16, *g = 1;
+    } else if (W <= 32) {
+        *wpl = 32, *g = 1;
+    } else if (W <= 64) {
+        *wpl = 64, *g = 1;
+    } else {
+        int G = 2;
+        while ((size_t)G * 64 < W)
+            G *= 2;
+        if (G > 32)
+            return fail(BMM_EINVAL, "gray search: rows wider than 2048 words are not supported");
+        *wpl = 64, *g = G;
+    }
+    return BMM_OK;
+}
+
+template <typename F>
+int dispatch_wg(int wpl, int g, F&& f) {
+#define BMM_WG(A, B)                                                                              \
+    if (wpl == A && g == B)                                                                       \
+        return f(std::integral_constant<int, A>{}, std::integral_constant<int, B>{});
+    BMM_WG(2, 1)
+    BMM_WG(4, 1)
+    BMM_WG(8, 1)
+    BMM_WG(16, 1)
+    BMM_WG(32, 1)
+    BMM_WG(64, 1)
+    BMM_WG(64, 2)
+    BMM_WG(64, 4)
+    BMM_WG(64, 8)
+    BMM_WG(64, 16)
+    BMM_WG(64, 32)
+#undef BMM_WG
+    return fail(BMM_EINVAL, "gray search: unsupported row shape");
+}
+
+template <typename F>
+int dispatch_e(int kk, F&& f) {
+    if (kk <= 32)
+        return f(std::integral_constant<int, 1>{});
+    if (kk <= 128)
+        return f(std::integral_constant<int, 4>{});
+    if (kk <= 1024)
+        return f(std::integral_constant<int, 32>{});
+    return fail(BMM_EINVAL, "gray search: k must be <= 1024");
+}
+
+}  // namespace
+
+int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items) {
+    // enough prefixes for ~8 resident CTAs of 128 threads per SM, with at
+    // least 2^6 Gray steps per prefix
+    const double want = (double)sm_count * 8 * kThreads / lanes_per_prefix / (n_items ? n_items : 1);
+    int hb = 0;
+    while (hb < t && (double)(1ull << hb) < want)
+        ++hb;
+    int chunk = t - hb;
+    if (chunk < 6)
+        chunk = t < 6 ? t : 6;
+    if (chunk > 20)
+        chunk = 20;
+    if (chunk > t)
+        chunk = t;
+    return chunk;
+}
+
+int gray_window_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, int chunk, int kk,
+                       bmm_candidate* d_out, cudaStream_t stream) {
+    int wpl = 0, g = 0;
+    BMM_TRY(group_shape((size_t)W, &wpl, &g));
+    const size_t srow_bytes = (size_t)t * wpl * g * 8;
+    const unsigned long long n_prefix = 1ull << (t - chunk);
+    return dispatch_wg(wpl, g, [&](auto WPLc, auto Gc) -> int {
+        constexpr int WPL = decltype(WPLc)::value, G = decltype(Gc)::value;
+        return dispatch_e(kk, [&](auto Ec) -> int {
+            constexpr int E = decltype(Ec)::value;
+            auto kern = gray_window_kernel<WPL, G, E>;
+            const size_t merge_bytes = (size_t)(kThreads / 32) * 32 * E * sizeof(bmm_candidate);
+            const size_t smem = srow_bytes > merge_bytes ? srow_bytes : merge_bytes;
+            if (smem > (size_t)ws->smem_optin)
+                return fail(BMM_EINVAL, "gray search: %zu bytes of rows exceed shared memory",
+                            srow_bytes);
+            BMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+            int occ = 0;
+            BMM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kThreads, smem));
+            if (occ < 1)
+                occ = 1;
+            unsigned long long need = (n_prefix * G + kThreads - 1) / kThreads;
+            unsigned long long grid = (unsigned long long)ws->sm_count * occ;
+            if (need < grid)
+                grid = need;
+            if (grid < 1)
+                grid = 1;
+            bmm_candidate* lists = nullptr;
+            BMM_TRY(ws_buffer(ws, kSlotCand, grid * kk * sizeof(bmm_candidate), (void**)&lists));
+            kern<<<(unsigned)grid, kThreads, smem, stream>>>(d_rows, t, W, chunk, n_prefix, kk,
+                                                            lists);
+            BMM_CUDA_TRY(cudaGetLastError());
+            return merge_topk_lists(lists, (int)grid, kk, d_out, stream);
+        });
+    });
+}
+
+int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int W,
+                        const uint32_t* d_targets, const uint32_t* d_others, int n_targets, int k,
+                        int tiebreak, int chunk, unsigned long long* d_keys, uint64_t* d_best_mask,
+                        uint32_t* d_best_weight, cudaStream_t stream) {
+    int wpl = 0, g = 0;
+    BMM_TRY(group_shape((size_t)W, &wpl, &g));
+    const size_t smem = (size_t)(k + 1) * wpl * g * 8;
+    if (smem > (size_t)ws->smem_optin)
+        return fail(BMM_EINVAL, "gray targets: %zu bytes of rows exceed shared memory", smem);
+    const unsigned long long n_prefix = 1ull << (k - chunk);
+    const unsigned long long per_cta = kThreads / g;
+    const unsigned long long ctas = (n_prefix + per_cta - 1) / per_cta;
+    if (ctas * (unsigned long long)n_targets > 0x7fffffffull)
+        return fail(BMM_EINVAL, "gray targets: grid too large (raise chunk_bits)");
+    BMM_CUDA_TRY(cudaMemsetAsync(d_keys, 0xff, sizeof(unsigned long long) * n_targets, stream));
+    BMM_TRY(dispatch_wg(wpl, g, [&](auto WPLc, auto Gc) -> int {
+        constexpr int WPL = decltype(WPLc)::value, G = decltype(Gc)::value;
+        auto kern = gray_targets_kernel<WPL, G>;
+        BMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+        kern<<<(unsigned)(ctas * n_targets), kThreads, smem, stream>>>(
+            d_words, stride, W, d_targets, d_others, k, chunk, tiebreak, (int)ctas, d_keys);
+        BMM_CUDA_TRY(cudaGetLastError());
+        return BMM_OK;
+    }));
+    decode_keys_kernel<<<(n_targets + 127) / 128, 128, 0, stream>>>(d_keys, n_targets, tiebreak,
+                                                                    d_best_mask, d_best_weight);
+    BMM_CUDA_TRY(cudaGetLastError());
+    return BMM_OK;
+}
+
+}  // namespace bmm

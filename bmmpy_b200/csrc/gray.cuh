@@ -1,0 +1,23 @@
+// Launchers for the Gray-code search kernels (gray.cu).  Device pointers,
+// asynchronous on `stream`.
+#pragma once
+
+#include "common.cuh"
+
+namespace bmm {
+
+// Low chunk width giving enough independent prefixes to fill the device.
+int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items);
+
+// Top-kk over all nonzero masks of the t rows in d_rows (t x W words).
+// d_out receives kk entries (empty ones have weight 0xffffffff).
+int gray_window_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, int chunk, int kk,
+                       bmm_candidate* d_out, cudaStream_t stream);
+
+// Per-target best (see bmm_gray_targets); d_keys is n_targets u64 scratch.
+int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int W,
+                        const uint32_t* d_targets, const uint32_t* d_others, int n_targets, int k,
+                        int tiebreak, int chunk, unsigned long long* d_keys, uint64_t* d_best_mask,
+                        uint32_t* d_best_weight, cudaStream_t stream);
+
+}  // namespace bmm

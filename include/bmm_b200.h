@@ -1,0 +1,151 @@
+/* bmm_b200.h -- C ABI of the B200 (sm_100a) weight-minimisation kernels.
+ *
+ * This is the drop-in boundary for bmmpy's search / FWHT / GA hot path.  It
+ * replaces the reference's launch seams and the bodies of its searcher
+ * classes (MortimerDe/bmmpy v0.5.3; citations are paths in that project):
+ *
+ *   bmm_fwht_search      FwhtSearch::search          src/search/fwht_search.cpp:34-132
+ *   bmm_mitm_search      MitmFwhtSearch::search      src/search/mitm_fwht_search.cpp:267-322
+ *                        CudaMitmFwhtSearch::search  src/search/cuda_mitm_fwht_search.cpp:123-180
+ *                        run_cuda_mitm_fwht_search   include/bmmpy/search/cuda_mitm_fwht_launch.hpp:15-16
+ *   bmm_gray_search      BruteforceSearch::search    src/search/bruteforce_search.cpp:300-329
+ *                        CudaBruteforceSearch::search src/search/cuda_bruteforce_search.cpp:38-103
+ *                        run_cuda_bruteforce_search  include/bmmpy/search/cuda_bruteforce_launch.hpp:22-23
+ *   bmm_fwht_i32/_i16    fwht_inplace                include/bmmpy/math/fwht.hpp:8-9
+ *   bmm_split_window     build_compact_split_window  include/bmmpy/search/split_window_prep.hpp:21-26
+ *   bmm_runtime_features get_runtime_features        include/bmmpy/stub.hpp:19-21
+ *   bmm_gray_targets / bmm_fwht_targets / bmm_batch_fwht_targets
+ *                        per-target form of the searches above: for target
+ *                        row i and k other rows, the reference window search
+ *                        over [i, o_1..o_k] restricted to masks with bit 0 set
+ *                        (best = (S << 1) | 1 in the reference's mask order).
+ *   bmm_ga_*             GeneticAlgorithm fitness evaluation and mutation
+ *                        src/ga/genetic_algorithm_internal.hpp:41-103,
+ *                        src/ga/genetic_algorithm_operators.cpp:100-192.
+ *
+ * Conventions
+ *  - Every function returns an int status (BMM_OK == 0, negative on error)
+ *    and never throws; bmm_last_error() gives the calling thread's message.
+ *    The status classes map to the reference's exception types:
+ *    BMM_EINVAL -> std::invalid_argument, BMM_EOVERFLOW -> std::overflow_error,
+ *    BMM_ECUDA / BMM_ENODEV / BMM_ETIMEOUT -> std::runtime_error.
+ *  - A matrix is row-major packed uint64 words: bit c of a row sits in word
+ *    c >> 6 at bit c & 63; `stride` words separate rows; bits at and past
+ *    `cols` must be zero (the reference BitMatrix layout).  A window is a list
+ *    of `t` row indices `win[0..t)`; mask bit j selects win[j].
+ *  - Functions without a suffix take HOST pointers, copy to the device,
+ *    run and copy back synchronously (the reference's calling convention).
+ *    Functions ending in _dev take DEVICE pointers and a cudaStream_t passed
+ *    as void*, are asynchronous, and never synchronise the device.
+ *  - Results are ordered by (weight ascending, mask ascending) -- the
+ *    reference's candidate_less -- and mask 0 is never reported by the
+ *    window searches.
+ *  - Calls from different host threads are safe; each thread owns its own
+ *    device workspace and stream per device.
+ */
+#ifndef BMM_B200_H
+#define BMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define BMM_API __attribute__((visibility("default")))
+#else
+#define BMM_API
+#endif
+
+#define BMM_OK 0
+#define BMM_EINVAL (-1)
+#define BMM_EOVERFLOW (-2)
+#define BMM_ECUDA (-3)
+#define BMM_ENODEV (-4)
+#define BMM_ETIMEOUT (-5)
+#define BMM_ENOMEM (-6)
+
+/* DeviceTopKEntry of include/bmmpy/search/cuda_launch_topk.cuh:11-14 (16 B). */
+typedef struct bmm_candidate {
+    uint64_t mask;
+    uint32_t weight;
+    uint32_t reserved;
+} bmm_candidate;
+
+/* RuntimeFeatures (include/bmmpy/stub.hpp:7-17), CUDA part. */
+typedef struct bmm_features {
+    int cuda_compiled;
+    int cuda_available;
+    int device_count;
+    int sm_count;      /* of the current device, 0 if none */
+    int cc_major;
+    int cc_minor;
+    char device_name[64];
+} bmm_features;
+
+/* Seeded synthetic instance (host memory, no device work): xorshift64
+ * (13, 7, 17; seed 0 -> 0x9E3779B97F4A7C15, include/bmmpy/core/detail/
+ * xorshift64.hpp:10-40) Bernoulli(p) fill, row-major with the column inner,
+ * bit = (next >> 11) * 2^-53 < p; then `scrambles` row XORs r_i ^= r_j with
+ * i = next % rows and j redrawn until j != i.  Returns the weight before
+ * scrambling (the planted weight). */
+BMM_API uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stride,
+                                  double p, uint64_t seed, size_t scrambles);
+
+BMM_API const char* bmm_last_error(void);
+BMM_API const char* bmm_version(void);
+BMM_API int bmm_runtime_features(bmm_features* out);
+
+/* ---- FWHT (fwht_inplace, include/bmmpy/math/fwht.hpp:8-9) ----
+ * Unnormalised Walsh-Hadamard transform in natural order with wrapping
+ * two's-complement add/sub; n must be a power of two (BMM_EINVAL otherwise);
+ * n <= 1 is a no-op. */
+BMM_API int bmm_fwht_i32(int32_t* data, size_t n);
+BMM_API int bmm_fwht_i16(int16_t* data, size_t n);
+BMM_API int bmm_fwht_i32_dev(int32_t* d_data, size_t n, void* stream);
+
+/* ---- window searches ----
+ * `out` holds room for `k` candidates; *out_count receives the number written
+ * (min(k, 2^t - 1)).  An empty result (t == 0, k == 0, cols == 0, or
+ * t > max_rows for bmm_fwht_search) is BMM_OK with *out_count == 0, as in the
+ * reference. */
+
+/* FwhtSearch: t <= min(max_rows, 30).  BMM_EOVERFLOW if the active column
+ * count exceeds INT32_MAX (fwht_search.cpp:77-87). */
+BMM_API int bmm_fwht_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
+                    size_t t, size_t max_rows, size_t k, bmm_candidate* out, size_t* out_count);
+
+/* Gray-code exhaustive search (BruteforceSearch / CudaBruteforceSearch).
+ * 1 <= t <= 64 (the enumeration must finish: t <= 44 in practice),
+ * k <= 1024, chunk_bits 0 (auto) or in [1, t] (as BruteforceSearch). */
+BMM_API int bmm_gray_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
+                    size_t t, size_t k, size_t chunk_bits, bmm_candidate* out,
+                    size_t* out_count);
+
+/* ---- per-target searches ----
+ * For each of n_targets targets: minimise popcount(row[targets[i]] ^ XOR of
+ * rows others[i*k + j] for j in S) over all S in [0, 2^k) (S = 0 included).
+ * best_mask[i] = S, best_weight[i] = that weight.  Ties: tiebreak 0 = the
+ * smallest S (the reference's mask order), 1 = the smallest reflected-Gray
+ * index of S.  Gray: k <= 40; FWHT: k <= 16 and cols <= 16383. */
+BMM_API int bmm_gray_targets(const uint64_t* words, size_t rows, size_t stride, size_t cols,
+                     const uint32_t* targets, const uint32_t* others, size_t n_targets, size_t k,
+                     int tiebreak, uint64_t* best_mask, uint32_t* best_weight);
+BMM_API int bmm_gray_targets_dev(const uint64_t* d_words, size_t rows, size_t stride, size_t cols,
+                         const uint32_t* d_targets, const uint32_t* d_others, size_t n_targets,
+                         size_t k, int tiebreak, uint64_t* d_best_mask, uint32_t* d_best_weight,
+                         void* stream);
+BMM_API int bmm_fwht_targets(const uint64_t* words, size_t rows, size_t stride, size_t cols,
+                     const uint32_t* targets, const uint32_t* others, size_t n_targets, size_t k,
+                     uint64_t* best_mask, uint32_t* best_weight);
+BMM_API int bmm_fwht_targets_dev(const uint64_t* d_words, size_t rows, size_t stride, size_t cols,
+                         const uint32_t* d_targets, const uint32_t* d_others, size_t n_targets,
+                         size_t k, uint64_t* d_best_mask, uint32_t* d_best_weight, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,584 @@
+/* CPU oracle: plain-C restatement of the reference hot path.  TEST
+ * INFRASTRUCTURE ONLY -- see bmm_oracle.h for the contract and the pinning.
+ * Each function names the reference file:line range it restates. */
+#include "bmm_oracle.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+#define WORD_BITS 64u
+
+static unsigned popc64(uint64_t x) { return (unsigned)__builtin_popcountll(x); }
+static unsigned ctz64(uint64_t x) { return (unsigned)__builtin_ctzll(x); }
+
+static uint64_t tail_mask_for_cols(size_t cols) {
+    /* src/search/fwht_search.cpp:24-30 */
+    const size_t tail = cols % WORD_BITS;
+    return tail == 0 ? ~(uint64_t)0 : (((uint64_t)1 << tail) - 1);
+}
+
+/* ---- xorshift64 (include/bmmpy/core/detail/xorshift64.hpp:10-40) ---- */
+uint64_t orc_xs_seed(uint64_t seed) { return seed == 0 ? 0x9E3779B97F4A7C15ull : seed; }
+
+uint64_t orc_xs_next(uint64_t* state) {
+    uint64_t x = *state;
+    x ^= x << 13;
+    x ^= x >> 7;
+    x ^= x << 17;
+    *state = x;
+    return x;
+}
+
+static size_t xs_index(uint64_t* state, size_t n) {
+    return n == 0 ? 0 : (size_t)(orc_xs_next(state) % n);
+}
+
+static double xs_unit(uint64_t* state) {
+    return (double)(orc_xs_next(state) >> 11) * (1.0 / 9007199254740992.0);
+}
+
+uint64_t orc_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stride, double p,
+                          uint64_t seed, size_t scrambles) {
+    uint64_t st = orc_xs_seed(seed);
+    uint64_t planted = 0;
+    memset(words, 0, rows * stride * sizeof(uint64_t));
+    for (size_t r = 0; r < rows; ++r)
+        for (size_t c = 0; c < cols; ++c)
+            if (xs_unit(&st) < p) {
+                words[r * stride + c / 64] |= (uint64_t)1 << (c % 64);
+                ++planted;
+            }
+    if (rows < 2)
+        return planted;
+    for (size_t s = 0; s < scrambles; ++s) {
+        const size_t i = xs_index(&st, rows);
+        size_t j = xs_index(&st, rows);
+        while (j == i)
+            j = xs_index(&st, rows);
+        for (size_t w = 0; w < stride; ++w)
+            words[i * stride + w] ^= words[j * stride + w];
+    }
+    return planted;
+}
+
+/* ---- FWHT (src/math/fwht.cpp:28-57, src/math/fwht_scalar.cpp:19-39) ---- */
+static int is_pow2(size_t n) { return n != 0 && (n & (n - 1)) == 0; }
+
+int orc_fwht_i32(int32_t* d, size_t n) {
+    if (n <= 1)
+        return 0;
+    if (!is_pow2(n))
+        return ORC_EINVAL;
+    for (size_t len = 1; len < n; len <<= 1)
+        for (size_t base = 0; base < n; base += 2 * len)
+            for (size_t i = 0; i < len; ++i) {
+                const uint32_t u = (uint32_t)d[base + i], v = (uint32_t)d[base + len + i];
+                d[base + i] = (int32_t)(u + v); /* two's-complement wrap */
+                d[base + len + i] = (int32_t)(u - v);
+            }
+    return 0;
+}
+
+int orc_fwht_i16(int16_t* d, size_t n) {
+    if (n <= 1)
+        return 0;
+    if (!is_pow2(n))
+        return ORC_EINVAL;
+    for (size_t len = 1; len < n; len <<= 1)
+        for (size_t base = 0; base < n; base += 2 * len)
+            for (size_t i = 0; i < len; ++i) {
+                const uint16_t u = (uint16_t)d[base + i], v = (uint16_t)d[base + len + i];
+                d[base + i] = (int16_t)(uint16_t)(u + v);
+                d[base + len + i] = (int16_t)(uint16_t)(u - v);
+            }
+    return 0;
+}
+
+/* ---- exact top-k by (weight asc, mask asc) ----
+ * Same order as candidate_less (src/search/fwht_search.cpp:15-22) and
+ * topk_less / insert_topk (src/search/bruteforce_search.cpp:29-54).  A bounded
+ * sorted insertion keeps exactly the k smallest pairs seen; mask 0 is never
+ * inserted. */
+typedef struct {
+    uint64_t* mask;
+    uint32_t* weight;
+    size_t size, k;
+} topk_t;
+
+static int pair_less(uint32_t wa, uint64_t ma, uint32_t wb, uint64_t mb) {
+    return wa < wb || (wa == wb && ma < mb);
+}
+
+static void topk_init(topk_t* t, size_t k) {
+    t->k = k;
+    t->size = 0;
+    t->mask = (uint64_t*)malloc((k ? k : 1) * sizeof(uint64_t));
+    t->weight = (uint32_t*)malloc((k ? k : 1) * sizeof(uint32_t));
+}
+
+static void topk_free(topk_t* t) {
+    free(t->mask);
+    free(t->weight);
+}
+
+static void topk_insert(topk_t* t, uint64_t mask, uint32_t w) {
+    if (mask == 0 || t->k == 0)
+        return;
+    if (t->size == t->k && !pair_less(w, mask, t->weight[t->size - 1], t->mask[t->size - 1]))
+        return;
+    /* lower_bound */
+    size_t lo = 0, hi = t->size;
+    while (lo < hi) {
+        const size_t mid = (lo + hi) / 2;
+        if (pair_less(t->weight[mid], t->mask[mid], w, mask))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    size_t last = t->size < t->k ? t->size : t->k - 1;
+    for (size_t i = last; i > lo; --i) {
+        t->mask[i] = t->mask[i - 1];
+        t->weight[i] = t->weight[i - 1];
+    }
+    t->mask[lo] = mask;
+    t->weight[lo] = w;
+    if (t->size < t->k)
+        ++t->size;
+}
+
+static long topk_emit(topk_t* t, uint64_t* out_mask, uint32_t* out_w, size_t cap) {
+    const size_t n = t->size < cap ? t->size : cap;
+    for (size_t i = 0; i < n; ++i) {
+        out_mask[i] = t->mask[i];
+        out_w[i] = t->weight[i];
+    }
+    const long count = (long)t->size;
+    topk_free(t);
+    return count;
+}
+
+/* Column pattern of window rows at word w, bit b. */
+static uint64_t col_pattern(const uint64_t* words, size_t stride, const size_t* win, size_t t,
+                            size_t w, unsigned b) {
+    uint64_t p = 0;
+    for (size_t r = 0; r < t; ++r)
+        if ((words[win[r] * stride + w] >> b) & 1u)
+            p |= (uint64_t)1 << r;
+    return p;
+}
+
+/* ---- FwhtSearch::search (src/search/fwht_search.cpp:34-132) ---- */
+long orc_fwht_search(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                     size_t t, size_t max_rows, size_t k, uint64_t* out_mask,
+                     uint32_t* out_weight, size_t cap) {
+    if (t == 0 || t > max_rows || k == 0) /* :36-37 */
+        return 0;
+    if (t > 64 || t >= 8 * sizeof(size_t)) /* :39-46 */
+        return ORC_EINVAL;
+    const size_t wpr = (cols + 63) / 64;
+    if (wpr == 0) /* :50-51 */
+        return 0;
+    const size_t n = (size_t)1 << t;
+    int32_t* h = (int32_t*)calloc(n, sizeof(int32_t));
+    if (!h)
+        return ORC_EINVAL;
+    uint64_t total = 0;
+    const uint64_t tail = tail_mask_for_cols(cols);
+    for (size_t w = 0; w < wpr; ++w) { /* :59-91 histogram of active columns */
+        uint64_t active = 0;
+        for (size_t r = 0; r < t; ++r)
+            active |= words[win[r] * stride + w];
+        if (w + 1 == wpr)
+            active &= tail;
+        while (active) {
+            const unsigned b = ctz64(active);
+            const uint64_t p = col_pattern(words, stride, win, t, w, b);
+            if (h[p] == INT32_MAX) {
+                free(h);
+                return ORC_EOVERFLOW;
+            }
+            ++h[p];
+            if (++total > (uint64_t)INT32_MAX) {
+                free(h);
+                return ORC_EOVERFLOW;
+            }
+            active &= active - 1;
+        }
+    }
+    orc_fwht_i32(h, n); /* :93 */
+    topk_t best;
+    topk_init(&best, k);
+    for (size_t mask = 1; mask < n; ++mask) { /* :105-126 */
+        const int64_t w2 = (int64_t)total - (int64_t)h[mask];
+        if (w2 < 0 || (w2 & 1))
+            continue;
+        topk_insert(&best, mask, (uint32_t)(w2 / 2));
+    }
+    free(h);
+    return topk_emit(&best, out_mask, out_weight, cap);
+}
+
+/* ---- build_compact_split_window (src/search/split_window_prep.cpp:42-137) ---- */
+static int cmp_u64(const void* a, const void* b) {
+    const uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+    return x < y ? -1 : (x > y);
+}
+
+long orc_split_window(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                      size_t t, size_t low_bits, uint64_t* q, uint64_t* r, int32_t* mult,
+                      size_t cap, int32_t* total_weight) {
+    if (low_bits > t || t > 64) /* :442-449 */
+        return ORC_EINVAL;
+    *total_weight = 0;
+    const size_t wpr = (cols + 63) / 64;
+    if (t == 0 || wpr == 0)
+        return 0;
+    uint64_t* pats = (uint64_t*)malloc((cols ? cols : 1) * sizeof(uint64_t));
+    size_t np = 0;
+    const uint64_t tail = tail_mask_for_cols(cols);
+    for (size_t w = 0; w < wpr; ++w) {
+        uint64_t active = 0;
+        for (size_t i = 0; i < t; ++i)
+            active |= words[win[i] * stride + w];
+        if (w + 1 == wpr)
+            active &= tail;
+        while (active) {
+            pats[np++] = col_pattern(words, stride, win, t, w, ctz64(active));
+            active &= active - 1;
+        }
+    }
+    if (np > (size_t)INT32_MAX) {
+        free(pats);
+        return ORC_EOVERFLOW;
+    }
+    *total_weight = (int32_t)np;
+    qsort(pats, np, sizeof(uint64_t), cmp_u64); /* sorted by pattern, :509-511 */
+    const uint64_t low_mask =
+        low_bits == 0 ? 0 : (low_bits >= 64 ? ~(uint64_t)0 : (((uint64_t)1 << low_bits) - 1));
+    size_t u = 0;
+    for (size_t i = 0; i < np;) {
+        size_t j = i;
+        while (j < np && pats[j] == pats[i])
+            ++j;
+        if (u < cap) {
+            q[u] = low_bits == 64 ? 0 : (pats[i] >> low_bits);
+            r[u] = pats[i] & low_mask;
+            mult[u] = (int32_t)(j - i);
+        }
+        ++u;
+        i = j;
+    }
+    free(pats);
+    return (long)u;
+}
+
+/* ---- MitmFwhtSearch::search (src/search/mitm_fwht_search.cpp) ---- */
+long orc_mitm_search(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                     size_t t, size_t k, uint64_t* out_mask, uint32_t* out_weight, size_t cap) {
+    if (k == 0 || t == 0) /* :270-275 */
+        return 0;
+    if (t > 64)
+        return ORC_EINVAL;
+    /* get_split_info :56-60 */
+    const size_t high = t <= 26 ? t / 2 : (t / 2 < 13 ? t / 2 : 13);
+    const size_t low = t - high;
+    if (low > 30 || low >= 31 || high >= 31) /* :283-289 */
+        return ORC_EINVAL;
+    const size_t wpr = (cols + 63) / 64;
+    size_t ucap = cols ? cols : 1;
+    uint64_t* q = (uint64_t*)malloc(ucap * sizeof(uint64_t));
+    uint64_t* r = (uint64_t*)malloc(ucap * sizeof(uint64_t));
+    int32_t* mult = (int32_t*)malloc(ucap * sizeof(int32_t));
+    int32_t total = 0;
+    long u = wpr ? orc_split_window(words, stride, cols, win, t, low, q, r, mult, ucap, &total) : 0;
+    if (u <= 0) {
+        free(q);
+        free(r);
+        free(mult);
+        return u < 0 ? u : 0;
+    }
+    /* build_adjacency :91-143: per low bit, the unique patterns whose r has it */
+    size_t* off = (size_t*)calloc(low + 1, sizeof(size_t));
+    for (long i = 0; i < u; ++i)
+        for (uint64_t m = r[i]; m; m &= m - 1)
+            ++off[ctz64(m) + 1];
+    for (size_t b = 0; b < low; ++b)
+        off[b + 1] += off[b];
+    size_t* cur = (size_t*)malloc((low + 1) * sizeof(size_t));
+    memcpy(cur, off, (low + 1) * sizeof(size_t));
+    int32_t* adj = (int32_t*)malloc((off[low] ? off[low] : 1) * sizeof(int32_t));
+    for (long i = 0; i < u; ++i)
+        for (uint64_t m = r[i]; m; m &= m - 1)
+            adj[cur[ctz64(m)]++] = (int32_t)i;
+    /* initialize_buckets :145-162 */
+    const size_t n_high = (size_t)1 << high;
+    int32_t* buckets = (int32_t*)calloc(n_high, sizeof(int32_t));
+    int32_t* tmp = (int32_t*)malloc(n_high * sizeof(int32_t));
+    int32_t* sgn = (int32_t*)malloc(u * sizeof(int32_t));
+    for (long i = 0; i < u; ++i) {
+        buckets[q[i]] += mult[i];
+        sgn[i] = mult[i];
+    }
+    topk_t best;
+    topk_init(&best, k);
+    const size_t n_loop = (size_t)1 << low;
+    uint64_t x_low = 0;
+    for (size_t i = 0; i < n_loop; ++i) {
+        if (i != 0) { /* apply_bit_flip :164-186 */
+            const size_t bit = ctz64(i);
+            for (size_t j = off[bit]; j < off[bit + 1]; ++j) {
+                const int32_t c = adj[j];
+                buckets[q[c]] -= 2 * sgn[c];
+                sgn[c] = -sgn[c];
+            }
+            x_low ^= (uint64_t)1 << bit;
+        }
+        /* process_candidate :233-265 */
+        memcpy(tmp, buckets, n_high * sizeof(int32_t));
+        orc_fwht_i32(tmp, n_high);
+        for (size_t xh = 0; xh < n_high; ++xh) {
+            const int64_t w2 = (int64_t)total - (int64_t)tmp[xh];
+            if (w2 < 0 || (w2 & 1))
+                continue;
+            const uint64_t mask = ((uint64_t)xh << low) | x_low;
+            if (mask)
+                topk_insert(&best, mask, (uint32_t)(w2 / 2));
+        }
+    }
+    free(q);
+    free(r);
+    free(mult);
+    free(off);
+    free(cur);
+    free(adj);
+    free(buckets);
+    free(tmp);
+    free(sgn);
+    return topk_emit(&best, out_mask, out_weight, cap);
+}
+
+/* ---- BruteforceSearch::search (src/search/bruteforce_search.cpp) ---- */
+long orc_bruteforce_search(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                           size_t t, size_t k, size_t chunk_bits, uint64_t* out_mask,
+                           uint32_t* out_weight, size_t cap) {
+    if (k == 0 || t == 0) /* :301-306 */
+        return 0;
+    if (t > 64)
+        return ORC_EINVAL;
+    const size_t wpr = (cols + 63) / 64;
+    if (wpr == 0)
+        return 0;
+    if (cols > (size_t)UINT32_MAX)
+        return ORC_EOVERFLOW;
+    /* resolve_chunk_bits :113-123 */
+    size_t chunk = chunk_bits;
+    if (chunk == 0)
+        chunk = t < 12 ? t : 12;
+    else if (chunk > t || chunk >= 64)
+        return ORC_EINVAL;
+    const size_t high_bits = t - chunk;
+    if (high_bits >= 63)
+        return ORC_EINVAL; /* the reference cannot enumerate this either */
+    const uint64_t prefixes = (uint64_t)1 << high_bits;
+    uint64_t* cur = (uint64_t*)malloc(wpr * sizeof(uint64_t));
+    topk_t best;
+    topk_init(&best, k);
+    for (uint64_t prefix = 0; prefix < prefixes; ++prefix) { /* sweep_prefix :126-170 */
+        memset(cur, 0, wpr * sizeof(uint64_t));
+        for (size_t hb = 0; hb < high_bits; ++hb)
+            if ((prefix >> hb) & 1u)
+                for (size_t w = 0; w < wpr; ++w)
+                    cur[w] ^= words[win[chunk + hb] * stride + w];
+        uint64_t mask = prefix << chunk;
+        uint32_t wt = 0;
+        for (size_t w = 0; w < wpr; ++w)
+            wt += popc64(cur[w]);
+        topk_insert(&best, mask, wt);
+        const uint64_t states = (uint64_t)1 << chunk;
+        for (uint64_t s = 1; s < states; ++s) {
+            const unsigned b = ctz64(s);
+            const uint64_t* row = words + win[b] * stride;
+            wt = 0;
+            for (size_t w = 0; w < wpr; ++w) {
+                cur[w] ^= row[w];
+                wt += popc64(cur[w]);
+            }
+            mask ^= (uint64_t)1 << b;
+            topk_insert(&best, mask, wt);
+        }
+    }
+    free(cur);
+    return topk_emit(&best, out_mask, out_weight, cap);
+}
+
+/* ---- per-target best ---- */
+static uint64_t inverse_gray(uint64_t s) {
+    for (unsigned sh = 1; sh < 64; sh <<= 1)
+        s ^= s >> sh;
+    return s;
+}
+
+int orc_target_best_gray(const uint64_t* words, size_t stride, size_t cols, size_t target,
+                         const size_t* others, size_t k, int tiebreak, uint64_t* best_mask,
+                         uint32_t* best_weight) {
+    if (k >= 63)
+        return ORC_EINVAL;
+    const size_t wpr = (cols + 63) / 64;
+    uint64_t* cur = (uint64_t*)malloc((wpr ? wpr : 1) * sizeof(uint64_t));
+    memcpy(cur, words + target * stride, wpr * sizeof(uint64_t));
+    uint32_t bw = 0;
+    for (size_t w = 0; w < wpr; ++w)
+        bw += popc64(cur[w]);
+    uint64_t bm = 0, bkey = 0, mask = 0;
+    const uint64_t states = (uint64_t)1 << k;
+    for (uint64_t s = 1; s < states; ++s) {
+        const unsigned b = ctz64(s);
+        const uint64_t* row = words + others[b] * stride;
+        uint32_t wt = 0;
+        for (size_t w = 0; w < wpr; ++w) {
+            cur[w] ^= row[w];
+            wt += popc64(cur[w]);
+        }
+        mask ^= (uint64_t)1 << b;
+        const uint64_t key = tiebreak ? s : mask; /* s == inverse_gray(mask) */
+        if (wt < bw || (wt == bw && key < bkey)) {
+            bw = wt;
+            bm = mask;
+            bkey = key;
+        }
+    }
+    (void)inverse_gray;
+    free(cur);
+    *best_mask = bm;
+    *best_weight = bw;
+    return 0;
+}
+
+int orc_target_best_fwht(const uint64_t* words, size_t stride, size_t cols, size_t target,
+                         const size_t* others, size_t k, uint64_t* best_mask,
+                         uint32_t* best_weight) {
+    if (k >= 31)
+        return ORC_EINVAL;
+    const size_t n = (size_t)1 << k;
+    int32_t* h = (int32_t*)calloc(n, sizeof(int32_t));
+    for (size_t c = 0; c < cols; ++c) {
+        uint64_t p = 0;
+        for (size_t j = 0; j < k; ++j)
+            if ((words[others[j] * stride + c / 64] >> (c % 64)) & 1u)
+                p |= (uint64_t)1 << j;
+        h[p] += ((words[target * stride + c / 64] >> (c % 64)) & 1u) ? -1 : 1;
+    }
+    orc_fwht_i32(h, n);
+    size_t best = 0;
+    for (size_t s = 1; s < n; ++s)
+        if (h[s] > h[best])
+            best = s;
+    *best_mask = best;
+    *best_weight = (uint32_t)(((int64_t)cols - h[best]) / 2);
+    free(h);
+    return 0;
+}
+
+/* ---- GA (src/ga/genetic_algorithm_internal.hpp:41-103) ---- */
+uint32_t orc_eval_cand_weight(const uint64_t* words, size_t stride, size_t cols,
+                              const size_t* win, size_t n, const uint64_t* mask, size_t mw) {
+    const size_t wpr = (cols + 63) / 64;
+    uint32_t total = 0;
+    const uint64_t tail = tail_mask_for_cols(cols);
+    for (size_t w = 0; w < wpr; ++w) {
+        uint64_t acc = 0;
+        for (size_t mi = 0; mi < mw; ++mi)
+            for (uint64_t m = mask[mi]; m; m &= m - 1) {
+                const size_t row = mi * 64 + ctz64(m);
+                if (row < n)
+                    acc ^= words[win[row] * stride + w];
+            }
+        if (w + 1 == wpr)
+            acc &= tail;
+        total += popc64(acc);
+    }
+    return total;
+}
+
+/* GeneticAlgorithm::mutate (src/ga/genetic_algorithm_operators.cpp:100-129) */
+void orc_mutate(const uint64_t* words, size_t stride, size_t cols, const size_t* win, size_t n,
+                uint64_t* masks, uint32_t* weights, size_t mw, double rate, uint64_t* rng_state) {
+    if (n < 2)
+        return;
+    size_t count = (size_t)((double)n * rate);
+    if (count < 1)
+        count = 1;
+    for (size_t c = 0; c < count; ++c) {
+        const size_t i = xs_index(rng_state, n);
+        const size_t j = xs_index(rng_state, n);
+        if (i == j)
+            continue;
+        for (size_t w = 0; w < mw; ++w)
+            masks[i * mw + w] ^= masks[j * mw + w];
+        weights[i] = orc_eval_cand_weight(words, stride, cols, win, n, masks + i * mw, mw);
+    }
+}
+
+/* GeneticAlgorithm::local_improvement (src/ga/genetic_algorithm_operators.cpp:131-192) */
+void orc_local_improvement(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                           size_t n, uint64_t* masks, uint32_t* weights, size_t mw) {
+    if (n < 2 || cols == 0)
+        return;
+    const size_t wpr = (cols + 63) / 64;
+    const uint64_t tail = tail_mask_for_cols(cols);
+    uint64_t* mat = (uint64_t*)calloc(n * wpr, sizeof(uint64_t));
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t w = 0; w < wpr; ++w) {
+            uint64_t acc = 0;
+            for (size_t mi = 0; mi < mw; ++mi)
+                for (uint64_t m = masks[i * mw + mi]; m; m &= m - 1) {
+                    const size_t row = mi * 64 + ctz64(m);
+                    if (row < n)
+                        acc ^= words[win[row] * stride + w];
+                }
+            if (w + 1 == wpr)
+                acc &= tail;
+            mat[i * wpr + w] = acc;
+        }
+        uint32_t wt = 0;
+        for (size_t w = 0; w < wpr; ++w)
+            wt += popc64(mat[i * wpr + w]);
+        weights[i] = wt;
+    }
+    for (int iter = 0; iter < 10; ++iter) {
+        int improved = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const uint64_t wi = weights[i];
+            if (wi == 0)
+                continue;
+            size_t best_j = n;
+            uint64_t best_w = wi;
+            for (size_t j = 0; j < n; ++j) {
+                if (i == j)
+                    continue;
+                const uint64_t wj = weights[j];
+                if (wj >= 2 * wi)
+                    continue;
+                uint64_t ov = 0;
+                for (size_t w = 0; w < wpr; ++w)
+                    ov += popc64(mat[i * wpr + w] & mat[j * wpr + w]);
+                const uint64_t cw = wi + wj - 2 * ov;
+                if (cw < best_w) {
+                    best_w = cw;
+                    best_j = j;
+                }
+            }
+            if (best_j == n)
+                continue;
+            for (size_t w = 0; w < mw; ++w)
+                masks[i * mw + w] ^= masks[best_j * mw + w];
+            for (size_t w = 0; w < wpr; ++w)
+                mat[i * wpr + w] ^= mat[best_j * wpr + w];
+            weights[i] = (uint32_t)best_w;
+            improved = 1;
+        }
+        if (!improved)
+            break;
+    }
+    free(mat);
+}

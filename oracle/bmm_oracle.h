@@ -1,0 +1,106 @@
+/* CPU oracle: a plain-C restatement of the reference's weight-minimisation
+ * hot path (MortimerDe/bmmpy v0.5.3).  TEST INFRASTRUCTURE ONLY: the tests,
+ * __graft_entry__.smoke() and bench.py's CPU baseline leg use it as the
+ * checker; the product never links or calls it.
+ *
+ * Parity is pinned two ways (see tests/test_oracle.py): against the reference
+ * library itself compiled from its own sources (oracle/_ref/libbmmref.so) and
+ * against the reference's known-answer tests, committed as golden vectors
+ * under tests/golden/.
+ *
+ * Matrix layout everywhere: row-major uint64 words, bit c of a row in word
+ * c>>6 at bit c&63, `stride` words between rows, bits past `cols` zero
+ * (include/bmmpy/core/bit_matrix.hpp:27-127, src/core/bit_matrix.cpp:67-72).
+ *
+ * Error returns mirror the reference exceptions: ORC_EINVAL for
+ * std::invalid_argument, ORC_EOVERFLOW for std::overflow_error.
+ */
+#ifndef BMM_ORACLE_H
+#define BMM_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_EINVAL (-1)
+#define ORC_EOVERFLOW (-2)
+
+/* xorshift64 (13, 7, 17); seed 0 maps to 0x9E3779B97F4A7C15
+ * (include/bmmpy/core/detail/xorshift64.hpp:10-40). */
+uint64_t orc_xs_next(uint64_t* state);
+uint64_t orc_xs_seed(uint64_t seed);
+
+/* Seeded synthetic instance: Bernoulli(p) fill (row-major, column inner,
+ * bit = unit_double < p), then `scrambles` row XORs r_i ^= r_j with
+ * i = next_index(rows), j redrawn until j != i.  Returns the planted weight
+ * (weight before scrambling). */
+uint64_t orc_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stride, double p,
+                          uint64_t seed, size_t scrambles);
+
+/* Unnormalised in-place Walsh-Hadamard transform with wrapping add/sub
+ * (src/math/fwht.cpp:28-57, src/math/fwht_scalar.cpp:19-39). */
+int orc_fwht_i32(int32_t* data, size_t n);
+int orc_fwht_i16(int16_t* data, size_t n);
+
+/* FwhtSearch::search (src/search/fwht_search.cpp:34-132): top-k (weight asc,
+ * mask asc) over every nonzero mask of the window rows `win[0..t)`.  Writes
+ * min(count, cap) results; returns count or a negative error. */
+long orc_fwht_search(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                     size_t t, size_t max_rows, size_t k, uint64_t* out_mask,
+                     uint32_t* out_weight, size_t cap);
+
+/* build_compact_split_window (src/search/split_window_prep.cpp:42-137):
+ * unique column patterns sorted ascending, split into q = p >> low and
+ * r = p & lowmask, with multiplicities.  Returns the unique count. */
+long orc_split_window(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                      size_t t, size_t low_bits, uint64_t* q, uint64_t* r, int32_t* mult,
+                      size_t cap, int32_t* total_weight);
+
+/* MitmFwhtSearch::search (src/search/mitm_fwht_search.cpp:56-60,91-186,233-322). */
+long orc_mitm_search(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                     size_t t, size_t k, uint64_t* out_mask, uint32_t* out_weight, size_t cap);
+
+/* BruteforceSearch::search (src/search/bruteforce_search.cpp:113-170,300-329). */
+long orc_bruteforce_search(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                           size_t t, size_t k, size_t chunk_bits, uint64_t* out_mask,
+                           uint32_t* out_weight, size_t cap);
+
+/* Per-target best XOR combination: minimise popcount(row[target] ^ XOR of
+ * rows others[j] for j in S) over all S (S = 0 included).  Reflected-Gray
+ * enumeration as in the reference's sweep (src/search/bruteforce_search.cpp:
+ * 157-169).  tiebreak 0: smallest S (the reference's (weight, mask) order,
+ * since its window mask is (S<<1)|1); tiebreak 1: smallest Gray index. */
+int orc_target_best_gray(const uint64_t* words, size_t stride, size_t cols, size_t target,
+                         const size_t* others, size_t k, int tiebreak, uint64_t* best_mask,
+                         uint32_t* best_weight);
+
+/* The same answer (tiebreak 0) through the signed column histogram and one
+ * 2^k-point transform: weight(S) = (cols - WHT[S]) / 2. */
+int orc_target_best_fwht(const uint64_t* words, size_t stride, size_t cols, size_t target,
+                         const size_t* others, size_t k, uint64_t* best_mask,
+                         uint32_t* best_weight);
+
+/* Genetic-algorithm kernels (src/ga/genetic_algorithm_internal.hpp:41-103,
+ * src/ga/genetic_algorithm_operators.cpp:100-192).  An individual is n
+ * candidate masks of mw = ceil(n/64) words each over the n window rows. */
+uint32_t orc_eval_cand_weight(const uint64_t* words, size_t stride, size_t cols,
+                              const size_t* win, size_t n, const uint64_t* mask, size_t mw);
+
+/* GeneticAlgorithm::mutate: count = max(1, floor(n*rate)) pair draws (i, j)
+ * from the xorshift state; i != j: mask_i ^= mask_j and re-score i. */
+void orc_mutate(const uint64_t* words, size_t stride, size_t cols, const size_t* win, size_t n,
+                uint64_t* masks, uint32_t* weights, size_t mw, double rate, uint64_t* rng_state);
+
+/* GeneticAlgorithm::local_improvement: materialise, then up to 10 greedy
+ * pairwise passes. */
+void orc_local_improvement(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                           size_t n, uint64_t* masks, uint32_t* weights, size_t mw);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

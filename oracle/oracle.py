@@ -1,0 +1,331 @@
+"""ctypes front-end for the two CPU checkers (test infrastructure only).
+
+* :data:`port` -- the plain-C restatement in ``oracle/bmm_oracle.c``
+  (``oracle/liboracle.so``), always available once ``make -C oracle`` ran.
+* :func:`ref` -- the unmodified reference C++ library compiled from its own
+  sources by ``make -C oracle ref`` (``oracle/_ref/libbmmref.so``); ``None``
+  where it was not built.
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py``
+import this module; the product never does.  Matrices are numpy ``uint64``
+arrays of shape ``(rows, stride)`` in the reference's packed layout.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libbmmref.so")
+
+_u64p = C.POINTER(C.c_uint64)
+_u32p = C.POINTER(C.c_uint32)
+_i32p = C.POINTER(C.c_int32)
+_i16p = C.POINTER(C.c_int16)
+_szp = C.POINTER(C.c_size_t)
+_sz = C.c_size_t
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+ERRORS = {-1: ValueError, -2: OverflowError, -3: IndexError, -4: RuntimeError, -5: RuntimeError}
+
+
+def _ptr(a, typ):
+    return a.ctypes.data_as(typ)
+
+
+def _build_port():
+    if not os.path.exists(PORT_SO):
+        subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+
+
+def _load_port():
+    _build_port()
+    lib = C.CDLL(PORT_SO)
+    lib.orc_gen_instance.restype = C.c_uint64
+    lib.orc_gen_instance.argtypes = [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz]
+    lib.orc_fwht_i32.argtypes = [_i32p, _sz]
+    lib.orc_fwht_i16.argtypes = [_i16p, _sz]
+    for name in ("orc_fwht_search",):
+        getattr(lib, name).restype = C.c_long
+        getattr(lib, name).argtypes = [_u64p, _sz, _sz, _szp, _sz, _sz, _sz, _u64p, _u32p, _sz]
+    lib.orc_mitm_search.restype = C.c_long
+    lib.orc_mitm_search.argtypes = [_u64p, _sz, _sz, _szp, _sz, _sz, _u64p, _u32p, _sz]
+    lib.orc_bruteforce_search.restype = C.c_long
+    lib.orc_bruteforce_search.argtypes = [_u64p, _sz, _sz, _szp, _sz, _sz, _sz, _u64p, _u32p, _sz]
+    lib.orc_split_window.restype = C.c_long
+    lib.orc_split_window.argtypes = [_u64p, _sz, _sz, _szp, _sz, _sz, _u64p, _u64p, _i32p, _sz, _i32p]
+    lib.orc_target_best_gray.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, C.c_int, _u64p, _u32p]
+    lib.orc_target_best_fwht.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _u64p, _u32p]
+    lib.orc_eval_cand_weight.restype = C.c_uint32
+    lib.orc_eval_cand_weight.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p, _sz]
+    lib.orc_mutate.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, _sz, C.c_double, _u64p]
+    lib.orc_local_improvement.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, _sz]
+    return lib
+
+
+class _Searches:
+    """Common window-search calls over either checker library."""
+
+    prefix = ""
+
+    def __init__(self, lib):
+        self.lib = lib
+
+    def _win(self, win):
+        return np.ascontiguousarray(np.asarray(win, dtype=np.uintp))
+
+    def _result(self, count, masks, weights):
+        if count < 0:
+            raise ERRORS.get(count, OracleError)(f"checker error {count}")
+        n = min(count, len(masks))
+        return [(int(masks[i]), int(weights[i])) for i in range(n)]
+
+
+class Port(_Searches):
+    def __init__(self):
+        super().__init__(_load_port())
+
+    def gen_instance(self, rows, cols, p, seed, scrambles=0, stride=None):
+        stride = stride or max(4, ((cols + 63) // 64 + 3) // 4 * 4)
+        m = np.zeros((rows, stride), dtype=np.uint64)
+        planted = self.lib.orc_gen_instance(_ptr(m, _u64p), rows, cols, stride, p, seed, scrambles)
+        return m, int(planted)
+
+    def fwht_i32(self, a):
+        a = np.ascontiguousarray(a, dtype=np.int32).copy()
+        rc = self.lib.orc_fwht_i32(_ptr(a, _i32p), a.size)
+        if rc:
+            raise ValueError("size must be a power of two")
+        return a
+
+    def fwht_i16(self, a):
+        a = np.ascontiguousarray(a, dtype=np.int16).copy()
+        rc = self.lib.orc_fwht_i16(_ptr(a, _i16p), a.size)
+        if rc:
+            raise ValueError("size must be a power of two")
+        return a
+
+    def fwht_search(self, m, cols, win, max_rows=16, k=64):
+        win = self._win(win)
+        cap = max(1, min(k, 1 << min(len(win), 24)))
+        masks = np.zeros(cap, np.uint64)
+        ws = np.zeros(cap, np.uint32)
+        c = self.lib.orc_fwht_search(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp), len(win),
+                                     max_rows, k, _ptr(masks, _u64p), _ptr(ws, _u32p), cap)
+        return self._result(c, masks, ws)
+
+    def mitm_search(self, m, cols, win, k=64):
+        win = self._win(win)
+        cap = max(1, min(k, 1 << min(len(win), 24)))
+        masks = np.zeros(cap, np.uint64)
+        ws = np.zeros(cap, np.uint32)
+        c = self.lib.orc_mitm_search(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp), len(win),
+                                     k, _ptr(masks, _u64p), _ptr(ws, _u32p), cap)
+        return self._result(c, masks, ws)
+
+    def bruteforce_search(self, m, cols, win, k=128, chunk_bits=0):
+        win = self._win(win)
+        cap = max(1, min(k, 1 << min(len(win), 24)))
+        masks = np.zeros(cap, np.uint64)
+        ws = np.zeros(cap, np.uint32)
+        c = self.lib.orc_bruteforce_search(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp),
+                                           len(win), k, chunk_bits, _ptr(masks, _u64p),
+                                           _ptr(ws, _u32p), cap)
+        return self._result(c, masks, ws)
+
+    def split_window(self, m, cols, win, low_bits):
+        win = self._win(win)
+        cap = max(1, cols)
+        q = np.zeros(cap, np.uint64)
+        r = np.zeros(cap, np.uint64)
+        mult = np.zeros(cap, np.int32)
+        tw = C.c_int32(0)
+        u = self.lib.orc_split_window(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp), len(win),
+                                      low_bits, _ptr(q, _u64p), _ptr(r, _u64p), _ptr(mult, _i32p),
+                                      cap, C.byref(tw))
+        if u < 0:
+            raise ERRORS.get(u, OracleError)(f"checker error {u}")
+        return q[:u].tolist(), r[:u].tolist(), mult[:u].tolist(), tw.value
+
+    def target_best_gray(self, m, cols, target, others, tiebreak=0):
+        others = self._win(others)
+        bm = C.c_uint64(0)
+        bw = C.c_uint32(0)
+        rc = self.lib.orc_target_best_gray(_ptr(m, _u64p), m.shape[1], cols, target,
+                                           _ptr(others, _szp), len(others), tiebreak,
+                                           C.byref(bm), C.byref(bw))
+        if rc:
+            raise ValueError("k too large")
+        return int(bm.value), int(bw.value)
+
+    def target_best_fwht(self, m, cols, target, others):
+        others = self._win(others)
+        bm = C.c_uint64(0)
+        bw = C.c_uint32(0)
+        rc = self.lib.orc_target_best_fwht(_ptr(m, _u64p), m.shape[1], cols, target,
+                                           _ptr(others, _szp), len(others), C.byref(bm), C.byref(bw))
+        if rc:
+            raise ValueError("k too large")
+        return int(bm.value), int(bw.value)
+
+    def eval_cand_weight(self, m, cols, win, mask_words):
+        win = self._win(win)
+        mk = np.ascontiguousarray(mask_words, dtype=np.uint64)
+        return int(self.lib.orc_eval_cand_weight(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp),
+                                                 len(win), _ptr(mk, _u64p), mk.size))
+
+    def mutate(self, m, cols, win, masks, weights, rate, rng_state):
+        """masks: (n, mw) uint64 (modified in place); returns new rng state."""
+        win = self._win(win)
+        st = C.c_uint64(rng_state)
+        self.lib.orc_mutate(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp), len(win),
+                            _ptr(masks, _u64p), _ptr(weights, _u32p), masks.shape[1], rate,
+                            C.byref(st))
+        return int(st.value)
+
+    def local_improvement(self, m, cols, win, masks, weights):
+        win = self._win(win)
+        self.lib.orc_local_improvement(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp),
+                                       len(win), _ptr(masks, _u64p), _ptr(weights, _u32p),
+                                       masks.shape[1])
+
+
+class Ref(_Searches):
+    """The reference library itself (oracle/_ref/libbmmref.so)."""
+
+    def __init__(self, lib):
+        super().__init__(lib)
+        L = lib
+        L.refh_fwht_i32.restype = C.c_long
+        L.refh_fwht_i32.argtypes = [_i32p, _sz]
+        L.refh_fwht_i16.restype = C.c_long
+        L.refh_fwht_i16.argtypes = [_i16p, _sz]
+        L.refh_fwht_search.restype = C.c_long
+        L.refh_fwht_search.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _u64p, _u32p, _sz]
+        L.refh_mitm_search.restype = C.c_long
+        L.refh_mitm_search.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _u64p, _u32p, _sz]
+        L.refh_bruteforce_search.restype = C.c_long
+        L.refh_bruteforce_search.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _u64p,
+                                             _u32p, _sz]
+        L.refh_split_window.restype = C.c_long
+        L.refh_split_window.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _u64p, _u64p, _i32p,
+                                        _sz, _i32p]
+        L.refh_target_best_fwht.restype = C.c_long
+        L.refh_target_best_fwht.argtypes = [_u64p, _sz, _sz, _sz, _sz, _szp, _sz, _u64p, _u32p]
+        L.refh_ga_run.restype = C.c_long
+        L.refh_ga_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_double,
+                                  C.c_uint64, _sz, C.c_uint64, _u64p, C.POINTER(C.c_double)]
+        L.refh_island_run.restype = C.c_long
+        L.refh_island_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_uint64,
+                                      _sz, C.c_uint64, C.c_double, _u64p, C.POINTER(C.c_double)]
+
+    def fwht_i32(self, a):
+        a = np.ascontiguousarray(a, dtype=np.int32).copy()
+        rc = self.lib.refh_fwht_i32(_ptr(a, _i32p), a.size)
+        if rc:
+            raise ERRORS.get(rc, OracleError)("reference error")
+        return a
+
+    def fwht_i16(self, a):
+        a = np.ascontiguousarray(a, dtype=np.int16).copy()
+        rc = self.lib.refh_fwht_i16(_ptr(a, _i16p), a.size)
+        if rc:
+            raise ERRORS.get(rc, OracleError)("reference error")
+        return a
+
+    def _call(self, fn, m, cols, win, k, *extra):
+        win = self._win(win)
+        cap = max(1, min(k, 1 << min(len(win), 24)))
+        masks = np.zeros(cap, np.uint64)
+        ws = np.zeros(cap, np.uint32)
+        c = fn(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], _ptr(win, _szp), len(win), *extra,
+               _ptr(masks, _u64p), _ptr(ws, _u32p), cap)
+        return self._result(c, masks, ws)
+
+    def fwht_search(self, m, cols, win, max_rows=16, k=64):
+        return self._call(self.lib.refh_fwht_search, m, cols, win, k, max_rows, k)
+
+    def mitm_search(self, m, cols, win, k=64):
+        return self._call(self.lib.refh_mitm_search, m, cols, win, k, k)
+
+    def bruteforce_search(self, m, cols, win, k=128, chunk_bits=0):
+        return self._call(self.lib.refh_bruteforce_search, m, cols, win, k, k, chunk_bits)
+
+    def split_window(self, m, cols, win, low_bits):
+        win = self._win(win)
+        cap = max(1, cols)
+        q = np.zeros(cap, np.uint64)
+        r = np.zeros(cap, np.uint64)
+        mult = np.zeros(cap, np.int32)
+        tw = C.c_int32(0)
+        u = self.lib.refh_split_window(_ptr(m, _u64p), m.shape[0], cols, m.shape[1],
+                                       _ptr(win, _szp), len(win), low_bits, _ptr(q, _u64p),
+                                       _ptr(r, _u64p), _ptr(mult, _i32p), cap, C.byref(tw))
+        if u < 0:
+            raise ERRORS.get(u, OracleError)(f"reference error {u}")
+        return q[:u].tolist(), r[:u].tolist(), mult[:u].tolist(), tw.value
+
+    def target_best_fwht(self, m, cols, target, others):
+        others = self._win(others)
+        bm = C.c_uint64(0)
+        bw = C.c_uint32(0)
+        rc = self.lib.refh_target_best_fwht(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], target,
+                                            _ptr(others, _szp), len(others), C.byref(bm),
+                                            C.byref(bw))
+        if rc < 0:
+            raise ERRORS.get(rc, OracleError)("reference error")
+        return int(bm.value), int(bw.value)
+
+    def ga_run(self, m, cols, win, population, elite, tournament, rate, seed, gens, target=0):
+        win = self._win(win)
+        scores = np.zeros(gens + 1, np.uint64)
+        secs = C.c_double(0)
+        g = self.lib.refh_ga_run(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], _ptr(win, _szp),
+                                 len(win), population, elite, tournament, rate, seed, gens, target,
+                                 _ptr(scores, _u64p), C.byref(secs))
+        if g < 0:
+            raise ERRORS.get(g, OracleError)("reference error")
+        return scores[: g + 1].tolist(), secs.value
+
+    def island_run(self, m, cols, win, islands, population, interval, seed, max_gens, target,
+                   cap_seconds):
+        win = self._win(win)
+        best = C.c_uint64(0)
+        secs = C.c_double(0)
+        rc = self.lib.refh_island_run(_ptr(m, _u64p), m.shape[0], cols, m.shape[1],
+                                      _ptr(win, _szp), len(win), islands, population, interval,
+                                      seed, max_gens, target, cap_seconds, C.byref(best),
+                                      C.byref(secs))
+        if rc < 0:
+            raise ERRORS.get(rc, OracleError)("reference error")
+        return int(best.value), secs.value
+
+
+_port = None
+
+
+def port() -> Port:
+    global _port
+    if _port is None:
+        _port = Port()
+    return _port
+
+
+_ref = None
+
+
+def ref():
+    """The reference library, or None where oracle/_ref was not built."""
+    global _ref
+    if _ref is None and os.path.exists(REF_SO):
+        _ref = Ref(C.CDLL(REF_SO))
+    return _ref

@@ -1,0 +1,287 @@
+// Test-infrastructure harness around the UNMODIFIED reference C++ sources.
+//
+// This file is part of the oracle: it is linked against the reference's own
+// translation units (compiled in place by oracle/Makefile into oracle/_ref/)
+// and exposes a handful of extern "C" shims so that the Python tests, the
+// golden-fixture generator and bench.py's reference arm can call the
+// reference implementation directly.  Nothing in the product links it.
+//
+// Every shim builds a reference `bmmpy::BitMatrix` from a packed row-major
+// uint64 buffer (bit c of a row in word c/64, bit c%64; `stride` words per
+// row) and calls the reference class named in its comment.
+//
+// Return convention: >= 0 on success (count of results written), negative on
+// a reference exception: -1 std::invalid_argument, -2 std::overflow_error,
+// -3 std::out_of_range, -4 std::logic_error, -5 other std::exception.
+
+#include "bmmpy/core/bit_matrix.hpp"
+#include "bmmpy/core/row_window.hpp"
+#include "bmmpy/ga/genetic_algorithm.hpp"
+#include "bmmpy/ga/island_model.hpp"
+#include "bmmpy/ga/migration/bounded_channel.hpp"
+#include "bmmpy/math/fwht.hpp"
+#include "bmmpy/search/bruteforce_search.hpp"
+#include "bmmpy/search/fwht_search.hpp"
+#include "bmmpy/search/mitm_fwht_search.hpp"
+#include "bmmpy/search/split_window_prep.hpp"
+
+#include <chrono>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <thread>
+#include <vector>
+
+namespace {
+
+bmmpy::BitMatrix make_matrix(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                             std::size_t stride) {
+    bmmpy::BitMatrix m(rows, cols);
+    const std::size_t wpr = m.words_per_row();
+    for (std::size_t r = 0; r < rows; ++r) {
+        std::uint64_t* dst = m.row_words(r);
+        for (std::size_t w = 0; w < wpr; ++w)
+            dst[w] = words[r * stride + w];
+        // keep the reference's invariant: bits past `cols` are zero
+        const std::size_t tail = cols % 64;
+        if (tail != 0 && wpr != 0)
+            dst[wpr - 1] &= (std::uint64_t{1} << tail) - 1;
+    }
+    return m;
+}
+
+template <typename Fn> long guarded(Fn&& fn) {
+    try {
+        return fn();
+    } catch (const std::invalid_argument&) {
+        return -1;
+    } catch (const std::overflow_error&) {
+        return -2;
+    } catch (const std::out_of_range&) {
+        return -3;
+    } catch (const std::logic_error&) {
+        return -4;
+    } catch (const std::exception&) {
+        return -5;
+    }
+}
+
+long emit(const std::vector<bmmpy::Candidate>& cands, std::size_t cap, std::uint64_t* out_mask,
+          std::uint32_t* out_weight) {
+    const std::size_t n = cands.size() < cap ? cands.size() : cap;
+    for (std::size_t i = 0; i < n; ++i) {
+        out_mask[i] = cands[i].mask_u64();
+        out_weight[i] = cands[i].weight;
+    }
+    return static_cast<long>(cands.size());
+}
+
+std::vector<std::size_t> to_rows(const std::size_t* win, std::size_t t) {
+    return std::vector<std::size_t>(win, win + t);
+}
+
+} // namespace
+
+extern "C" {
+
+// bmmpy::fwht_inplace(int32_t*, size_t)
+long refh_fwht_i32(std::int32_t* data, std::size_t n) {
+    return guarded([&] {
+        bmmpy::fwht_inplace(data, n);
+        return 0L;
+    });
+}
+
+// bmmpy::fwht_inplace(int16_t*, size_t)
+long refh_fwht_i16(std::int16_t* data, std::size_t n) {
+    return guarded([&] {
+        bmmpy::fwht_inplace(data, n);
+        return 0L;
+    });
+}
+
+// bmmpy::FwhtSearch{max_rows, k}.search(window)
+long refh_fwht_search(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                      std::size_t stride, const std::size_t* win, std::size_t t,
+                      std::size_t max_rows, std::size_t k, std::uint64_t* out_mask,
+                      std::uint32_t* out_weight, std::size_t cap) {
+    return guarded([&] {
+        const auto m = make_matrix(words, rows, cols, stride);
+        const auto w = m.row_window(to_rows(win, t));
+        bmmpy::FwhtSearch s(bmmpy::FwhtSearchConfig{max_rows, k});
+        return emit(s.search(w), cap, out_mask, out_weight);
+    });
+}
+
+// bmmpy::MitmFwhtSearch{..., k}.search(window)
+long refh_mitm_search(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                      std::size_t stride, const std::size_t* win, std::size_t t, std::size_t k,
+                      std::uint64_t* out_mask, std::uint32_t* out_weight, std::size_t cap) {
+    return guarded([&] {
+        const auto m = make_matrix(words, rows, cols, stride);
+        const auto w = m.row_window(to_rows(win, t));
+        bmmpy::MitmFwhtSearchConfig cfg;
+        cfg.max_candidates = k;
+        bmmpy::MitmFwhtSearch s(cfg);
+        return emit(s.search(w), cap, out_mask, out_weight);
+    });
+}
+
+// bmmpy::BruteforceSearch{k, chunk_bits}.search(window)
+long refh_bruteforce_search(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                            std::size_t stride, const std::size_t* win, std::size_t t,
+                            std::size_t k, std::size_t chunk_bits, std::uint64_t* out_mask,
+                            std::uint32_t* out_weight, std::size_t cap) {
+    return guarded([&] {
+        const auto m = make_matrix(words, rows, cols, stride);
+        const auto w = m.row_window(to_rows(win, t));
+        bmmpy::BruteforceSearch s(bmmpy::BruteforceSearchConfig{k, chunk_bits});
+        return emit(s.search(w), cap, out_mask, out_weight);
+    });
+}
+
+// bmmpy::build_compact_split_window(window, low_bits)
+long refh_split_window(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                       std::size_t stride, const std::size_t* win, std::size_t t,
+                       std::size_t low_bits, std::uint64_t* q, std::uint64_t* r,
+                       std::int32_t* mult, std::size_t cap, std::int32_t* total_weight) {
+    return guarded([&] {
+        const auto m = make_matrix(words, rows, cols, stride);
+        const auto w = m.row_window(to_rows(win, t));
+        const auto prep = bmmpy::build_compact_split_window(w, low_bits);
+        *total_weight = prep.total_weight;
+        const std::size_t n = prep.multiplicity.size();
+        for (std::size_t i = 0; i < n && i < cap; ++i) {
+            q[i] = prep.q[i];
+            r[i] = prep.r[i];
+            mult[i] = prep.multiplicity[i];
+        }
+        return static_cast<long>(n);
+    });
+}
+
+// Per-target best combination (weight of row_target XOR rows in S, all S over
+// `others`, S = 0 included, ties by smallest S) computed through the
+// reference's own bmmpy::fwht_inplace on the signed column histogram.  Used to
+// make golden vectors for the per-target workloads; the histogram fill is
+// harness code, the transform is the reference's.
+long refh_target_best_fwht(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                           std::size_t stride, std::size_t target, const std::size_t* others,
+                           std::size_t k, std::uint64_t* out_mask, std::uint32_t* out_weight) {
+    return guarded([&] {
+        if (k >= 31)
+            throw std::invalid_argument("refh_target_best_fwht: k too large");
+        const auto m = make_matrix(words, rows, cols, stride);
+        const std::size_t n = std::size_t{1} << k;
+        std::vector<std::int32_t> h(n, 0);
+        for (std::size_t c = 0; c < cols; ++c) {
+            std::size_t p = 0;
+            for (std::size_t j = 0; j < k; ++j)
+                if (m.get(others[j], c))
+                    p |= std::size_t{1} << j;
+            h[p] += m.get(target, c) ? -1 : 1;
+        }
+        bmmpy::fwht_inplace(h.data(), n);
+        std::size_t best = 0;
+        for (std::size_t s = 1; s < n; ++s)
+            if (h[s] > h[best])
+                best = s;
+        *out_mask = best;
+        *out_weight = static_cast<std::uint32_t>((static_cast<std::int64_t>(cols) - h[best]) / 2);
+        return 1L;
+    });
+}
+
+// Single-island bmmpy::ga::GeneticAlgorithm run; best_score after
+// initialize() and after each generation is written to scores[0..gens].
+long refh_ga_run(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                 std::size_t stride, const std::size_t* win, std::size_t t,
+                 std::size_t population, std::size_t elite, std::size_t tournament,
+                 double mutation_rate, std::uint64_t seed, std::size_t gens,
+                 std::uint64_t target_weight, std::uint64_t* scores, double* seconds) {
+    return guarded([&] {
+        const auto m = make_matrix(words, rows, cols, stride);
+        const auto w = m.row_window(to_rows(win, t));
+        bmmpy::ga::GeneticAlgorithmConfig cfg;
+        cfg.population_size = population;
+        cfg.elite_count = elite;
+        cfg.tournament_size = tournament;
+        cfg.mutation_rate = mutation_rate;
+        cfg.seed = seed;
+        cfg.stop.max_generations = gens;
+        if (target_weight != 0)
+            cfg.stop.target_total_weight = target_weight;
+        bmmpy::ga::GeneticAlgorithm ga(cfg);
+        const auto t0 = std::chrono::steady_clock::now();
+        ga.initialize(w);
+        scores[0] = ga.best_score();
+        std::size_t g = 0;
+        while (!ga.done()) {
+            ga.step();
+            ++g;
+            scores[g] = ga.best_score();
+        }
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return static_cast<long>(g);
+    });
+}
+
+// The reference bmmpy::ga::IslandModel (one std::thread per island, shared
+// BoundedChannel pool) run to completion with a wall-clock cap enforced by
+// request_stop().  Returns the best score; seconds receives the wall time.
+long refh_island_run(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                     std::size_t stride, const std::size_t* win, std::size_t t,
+                     std::size_t islands, std::size_t population, std::size_t interval,
+                     std::uint64_t seed, std::size_t max_gens, std::uint64_t target_weight,
+                     double cap_seconds, std::uint64_t* best_score, double* seconds) {
+    return guarded([&] {
+        const auto m = make_matrix(words, rows, cols, stride);
+        const auto w = m.row_window(to_rows(win, t));
+        bmmpy::ga::IslandModelConfig mc;
+        for (std::size_t i = 0; i < islands; ++i) {
+            bmmpy::ga::IslandSpec spec;
+            spec.island_id = i;
+            spec.migration.interval_generations = interval;
+            spec.migration.export_count = 1;
+            spec.migration.import_count = 1;
+            mc.islands.push_back(spec);
+        }
+        auto factory = [&](const bmmpy::ga::IslandSpec& spec) {
+            bmmpy::ga::GeneticAlgorithmConfig cfg;
+            cfg.population_size = population;
+            cfg.seed = seed + spec.island_id;
+            cfg.stop.max_generations = max_gens;
+            if (target_weight != 0)
+                cfg.stop.target_total_weight = target_weight;
+            return std::unique_ptr<bmmpy::ga::Algorithm>(new bmmpy::ga::GeneticAlgorithm(cfg));
+        };
+        bmmpy::ga::IslandModel model(
+            mc, factory, std::make_unique<bmmpy::ga::migration::BoundedChannel>(128));
+        const auto t0 = std::chrono::steady_clock::now();
+        model.initialize(w);
+        model.start();
+        while (model.running()) {
+            const auto snap = model.snapshot();
+            bool all_done = true;
+            for (const auto& is : snap.islands)
+                all_done = all_done && is.finished;
+            if (all_done)
+                break;
+            if (target_weight != 0 && snap.best_score <= target_weight)
+                break;
+            const double el =
+                std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+            if (el > cap_seconds)
+                break;
+            std::this_thread::sleep_for(std::chrono::milliseconds(20));
+        }
+        model.request_stop();
+        model.wait();
+        *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        *best_score = model.snapshot().best_score;
+        return 0L;
+    });
+}
+
+} // extern "C"

@@ -1,0 +1,176 @@
+"""CPU suite: the oracle (C restatement) is pinned to the reference.
+
+* against the reference's own known-answer tests and the golden vectors the
+  reference produced (tests/golden/, made by tests/golden/make_golden.py);
+* against the reference library itself (oracle/_ref) on random windows when
+  that library was built in this checkout.
+"""
+
+import json
+import os
+import random
+
+import numpy as np
+import pytest
+
+from oracle.oracle import port, ref
+from tests.golden.fixtures import (
+    C1,
+    C2,
+    batch_instance,
+    checksum_pairs,
+    cuda_equivalence_matrix,
+    matrix_from_rows,
+    python_random_matrix,
+)
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module")
+def ka():
+    with open(os.path.join(GOLDEN, "known_answers.json")) as f:
+        return json.load(f)
+
+
+@pytest.fixture(scope="module")
+def wl():
+    return np.load(os.path.join(GOLDEN, "workloads.npz"))
+
+
+def pairs(x):
+    return [tuple(map(int, p)) for p in x]
+
+
+def test_fwht_known_answers(ka):
+    P = port()
+    assert P.fwht_i32([1, 2, 3, 4]).tolist() == [10, -2, -4, 0] == ka["fwht_i32"]["expected"]
+    assert P.fwht_i16([32767, 1]).tolist() == [-32768, 32766] == ka["fwht_i16_wrap"]["expected"]
+    with pytest.raises(ValueError):
+        P.fwht_i32([1, 2, 3])
+
+
+def test_search_known_answers(ka):
+    P = port()
+    m, cols = matrix_from_rows(["10101", "10101"])
+    got = P.fwht_search(m, cols, [0, 1], 16, 64)
+    assert pairs(got) == pairs(ka["fwht_2x5_k64"])
+    assert got[0] == (3, 0) and len(got) == 3
+    assert pairs(P.fwht_search(m, cols, [0, 1], 16, 1)) == pairs(ka["fwht_2x5_k1"])
+    assert pairs(P.bruteforce_search(m, cols, [0, 1], 1, 0)) == pairs(ka["brute_2x5_k1"])
+    m, cols = matrix_from_rows(ka["six_rows"])
+    six = list(range(6))
+    assert pairs(P.fwht_search(m, cols, six, 16, 8)) == pairs(ka["fwht_6x12_k8"])
+    assert pairs(P.mitm_search(m, cols, six, 8)) == pairs(ka["mitm_6x12_k8"])
+    assert pairs(P.bruteforce_search(m, cols, six, 8, 0)) == pairs(ka["brute_6x12_k8"])
+    assert pairs(P.fwht_search(m, cols, six, 16, 63)) == pairs(ka["fwht_6x12_all"])
+    m, cols = matrix_from_rows(["10101", "11100", "00111"])
+    assert pairs(P.fwht_search(m, cols, [0, 1, 2], 16, 4)) == pairs(ka["fwht_3x5_k4"])
+
+
+def test_split_window_known_answer(ka):
+    m, cols = matrix_from_rows(["11001", "00100", "01101", "01001"])
+    q, r, mult, tw = port().split_window(m, cols, [0, 1, 2, 3], 2)
+    exp = ka["split_4x5_low2"]
+    assert (q, r, mult, tw) == (exp["q"], exp["r"], exp["mult"], exp["total_weight"])
+    assert (q, r, mult, tw) == ([0, 1, 3], [1, 2, 1], [1, 1, 2], 4)
+
+
+def test_cuda_equivalence_fixtures(ka):
+    P = port()
+    m, cols = cuda_equivalence_matrix(28, 96)
+    assert pairs(P.mitm_search(m, cols, list(range(28)), 8)) == pairs(ka["mitm_28x96_k8"])
+    for c, k in ((512, 8), (1024, 128)):
+        m, cols = cuda_equivalence_matrix(16, c)
+        got = P.bruteforce_search(m, cols, list(range(16)), k, 0)
+        assert pairs(got) == pairs(ka[f"brute_16x{c}_k{k}"])
+    m, cols = python_random_matrix(16, 512, 42)
+    assert pairs(P.bruteforce_search(m, cols, list(range(16)), 8, 0)) == pairs(
+        ka["brute_pyrand_16x512_k8"])
+
+
+def test_c1_golden(wl):
+    P = port()
+    m, _ = P.gen_instance(C1["rows"], C1["cols"], C1["p"], C1["seed"])
+    for i in range(C1["rows"]):
+        others = [(i + 1 + j) % C1["rows"] for j in range(C1["k"])]
+        f = P.target_best_fwht(m, C1["cols"], i, others)
+        assert f == (int(wl["c1_mask"][i]), int(wl["c1_weight"][i]))
+        if i < 4:
+            assert P.target_best_gray(m, C1["cols"], i, others) == f
+    # the per-target best is the reference window search's best mask with bit 0
+    mask, weight = (int(v) for v in wl["c1_row0_window_best"])
+    assert (mask, weight) == ((int(wl["c1_mask"][0]) << 1) | 1, int(wl["c1_weight"][0]))
+
+
+def test_c2_reduced_golden(wl):
+    P = port()
+    m, _ = P.gen_instance(C2["rows"], C2["cols"], C2["p"], C2["seed"])
+    for i in range(0, C2["rows"], 7):
+        others = [(i + 1 + j) % C2["rows"] for j in range(16)]
+        g = P.target_best_gray(m, C2["cols"], i, others)
+        assert g == (int(wl["c2k16_mask"][i]), int(wl["c2k16_weight"][i]))
+
+
+def test_c4_first_instances_golden(wl):
+    P = port()
+    first = wl["c4_first32"]
+    row = 0
+    for idx in range(8):
+        mm, n, cols, k, _ = batch_instance(P, idx)
+        ms, ws = [], []
+        for i in range(n):
+            others = [(i + 1 + j) % n for j in range(k)]
+            bm, bw = P.target_best_fwht(mm, cols, i, others)
+            ms.append(bm)
+            ws.append(bw)
+            assert (bm, bw) == (int(first[row][0]), int(first[row][1]))
+            row += 1
+        assert checksum_pairs(ms, ws) == int(wl["c4_checksums"][idx])
+
+
+def test_ga_kernels_small():
+    """mutate / local_improvement restatements keep their invariants."""
+    P = port()
+    m, _ = P.gen_instance(20, 150, 0.3, 9, 10)
+    win = list(range(20))
+    n, mw = 20, 1
+    masks = np.array([[1 << i] for i in range(n)], np.uint64)
+    weights = np.array([P.eval_cand_weight(m, 150, win, masks[i]) for i in range(n)], np.uint32)
+    st = P.mutate(m, 150, win, masks, weights, 0.3, 12345)
+    assert st != 12345
+    for i in range(n):
+        assert weights[i] == P.eval_cand_weight(m, 150, win, masks[i])
+    P.local_improvement(m, 150, win, masks, weights)
+    for i in range(n):
+        assert weights[i] == P.eval_cand_weight(m, 150, win, masks[i])
+
+
+@pytest.mark.skipif(ref() is None, reason="reference library not built (make -C oracle ref)")
+def test_port_matches_reference_random():
+    P, R = port(), ref()
+    rng = random.Random(7)
+    for trial in range(40):
+        rows = rng.randint(1, 18)
+        cols = rng.choice([1, 7, 64, 65, 200, 513])
+        m, _ = P.gen_instance(rows, cols, rng.choice([0.1, 0.5]), rng.randint(0, 1000),
+                              rng.randint(0, 5))
+        t = rng.randint(1, rows)
+        win = rng.sample(range(rows), t)
+        k = rng.choice([1, 3, 64, 500])
+        assert P.fwht_search(m, cols, win, 16, k) == R.fwht_search(m, cols, win, 16, k)
+        assert P.mitm_search(m, cols, win, k) == R.mitm_search(m, cols, win, k)
+        cb = rng.choice([0, 1, t])
+        assert P.bruteforce_search(m, cols, win, k, cb) == R.bruteforce_search(m, cols, win, k, cb)
+        lb = rng.randint(0, t)
+        assert P.split_window(m, cols, win, lb) == R.split_window(m, cols, win, lb)
+
+
+@pytest.mark.skipif(ref() is None, reason="reference library not built (make -C oracle ref)")
+def test_port_error_classes_match_reference():
+    P, R = port(), ref()
+    m, cols = matrix_from_rows(["101"] * 3)
+    with pytest.raises(ValueError):
+        R.bruteforce_search(m, cols, [0, 1, 2], 4, 5)
+    with pytest.raises(ValueError):
+        P.bruteforce_search(m, cols, [0, 1, 2], 4, 5)
