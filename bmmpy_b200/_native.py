@@ -43,6 +43,7 @@ _candp = C.POINTER(Candidate_t)
 # name -> argtypes (all return int unless listed in _RESTYPES)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
+    "bmm_probe_xor_popc": [C.POINTER(C.c_double)],
     "bmm_last_error": [],
     "bmm_version": [],
     "bmm_runtime_features": [C.POINTER(Features_t)],

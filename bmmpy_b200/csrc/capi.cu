@@ -127,10 +127,12 @@ int merge_topk_lists(const bmm_candidate* d_lists, int nlists, int kk, bmm_candi
     auto run = [&](auto Ec) -> int {
         constexpr int E = decltype(Ec)::value;
         auto mk = merge_lists_kernel<E>;
-        const size_t msmem = (size_t)32 * 32 * E * sizeof(bmm_candidate);
+        // every warp stages a 32*E list in shared memory: keep that under 128 KB
+        const int warps = E >= 32 ? 8 : 32;
+        const size_t msmem = (size_t)warps * 32 * E * sizeof(bmm_candidate);
         BMM_CUDA_TRY(
             cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
-        mk<<<1, 1024, msmem, stream>>>(d_lists, nlists, kk, d_out);
+        mk<<<1, warps * 32, msmem, stream>>>(d_lists, nlists, kk, d_out);
         BMM_CUDA_TRY(cudaGetLastError());
         return BMM_OK;
     };
@@ -265,6 +267,13 @@ uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stri
             words[i * stride + w] ^= words[j * stride + w];
     }
     return planted;
+}
+
+int bmm_probe_xor_popc(double* words_per_second) {
+    clear_error();
+    if (!words_per_second)
+        return fail(BMM_EINVAL, "null output");
+    return popc_probe(words_per_second);
 }
 
 const char* bmm_last_error(void) { return g_err; }

@@ -378,3 +378,55 @@ int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int 
 }
 
 }  // namespace bmm
+
+// ---------------------------------------------------------------------------
+// Throughput probe for the roofline denominator of the Gray-code kernels:
+// the same per-word work as a Gray step (64-bit XOR + 64-bit POPC + add)
+// with everything in registers (no shared-memory loads, no top-k), so its
+// rate is the device's ceiling for that instruction mix.
+namespace bmm {
+namespace {
+__global__ void __launch_bounds__(256) popc_probe_kernel(int iters, unsigned long long* sink) {
+    uint64_t x[64];
+#pragma unroll
+    for (int i = 0; i < 64; ++i)
+        x[i] = (uint64_t)(threadIdx.x + 1) * 0x9E3779B97F4A7C15ull + (uint64_t)i * 0x632BE59BD9B4E019ull;
+    uint32_t acc = 0;
+    uint64_t c = blockIdx.x;
+    for (int it = 0; it < iters; ++it) {
+        c = c * 6364136223846793005ull + 1442695040888963407ull;
+#pragma unroll
+        for (int i = 0; i < 64; ++i) {
+            x[i] ^= c;
+            acc += __popcll(x[i]);
+        }
+    }
+    if (acc == 0x7fffffffu)  // never true in practice; keeps the work alive
+        sink[blockIdx.x] = acc;
+}
+}  // namespace
+
+int popc_probe(double* words_per_second) {
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    void* sink = nullptr;
+    BMM_TRY(ws_buffer(ws, kSlotExtra1, 8 * 4096, &sink));
+    const int blocks = ws->sm_count * 4, iters = 4096;
+    cudaEvent_t a, b;
+    BMM_CUDA_TRY(cudaEventCreate(&a));
+    BMM_CUDA_TRY(cudaEventCreate(&b));
+    popc_probe_kernel<<<blocks, 256, 0, ws->stream>>>(64, (unsigned long long*)sink);  // warm
+    BMM_CUDA_TRY(cudaEventRecord(a, ws->stream));
+    popc_probe_kernel<<<blocks, 256, 0, ws->stream>>>(iters, (unsigned long long*)sink);
+    BMM_CUDA_TRY(cudaEventRecord(b, ws->stream));
+    BMM_CUDA_TRY(cudaEventSynchronize(b));
+    float ms = 0;
+    BMM_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *words_per_second = (double)blocks * 256 * iters * 64 / (ms * 1e-3);
+    return BMM_OK;
+}
+}  // namespace bmm

@@ -20,4 +20,7 @@ int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int 
                         int tiebreak, int chunk, unsigned long long* d_keys, uint64_t* d_best_mask,
                         uint32_t* d_best_weight, cudaStream_t stream);
 
+// Measures the register-only 64-bit XOR+POPC word rate of the device.
+int popc_probe(double* words_per_second);
+
 }  // namespace bmm

@@ -94,6 +94,12 @@ typedef struct bmm_features {
 BMM_API uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stride,
                                   double p, uint64_t seed, size_t scrambles);
 
+/* Roofline probe for the Gray-code kernels: runs a register-only kernel with
+ * the per-word work of one Gray step (64-bit XOR, 64-bit POPC, add) over the
+ * whole device and returns its rate in 64-bit words per second.  No
+ * reference counterpart (measurement aid). */
+BMM_API int bmm_probe_xor_popc(double* words_per_second);
+
 BMM_API const char* bmm_last_error(void);
 BMM_API const char* bmm_version(void);
 BMM_API int bmm_runtime_features(bmm_features* out);
