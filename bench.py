@@ -114,12 +114,15 @@ def clock_summary(sampler):
 
 def load_traffic():
     """dram bytes per launch of gray_targets_kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "gray_targets_c2.json")
+    path = os.path.join(ROOT, "profiles", "gray_targets_c2.md")
     try:
         with open(path) as f:
-            return json.load(f).get("dram_bytes_per_launch")
+            for ln in f:
+                if ln.startswith("dram_bytes_per_launch:"):
+                    return int(ln.split(":", 1)[1])
     except (OSError, ValueError):
-        return None
+        pass
+    return None
 
 
 # ---------------------------------------------------------------------------
