@@ -54,6 +54,7 @@ SIGNATURES = {
     "bmm_gray_search": [_u64p, _sz, _sz, _u32p, _sz, _sz, _sz, _candp, _szp],
     "bmm_gray_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, C.c_int, _u64p, _u32p],
     "bmm_gray_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, C.c_int, _vp, _vp, _vp],
+    "bmm_gray_targets_noalloc": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, C.c_int, _vp, _vp, _vp],
     "bmm_fwht_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, _u64p, _u32p],
     "bmm_fwht_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp, _vp],
 }

@@ -19,6 +19,8 @@
 #include "gray.cuh"
 #include "topk.cuh"
 
+#include <mutex>
+
 namespace bmm {
 namespace {
 
@@ -430,3 +432,110 @@ int popc_probe(double* words_per_second) {
     return BMM_OK;
 }
 }  // namespace bmm
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the per-target Gray-code search.
+//
+// Who needs it: callers that are not allowed to allocate device memory --
+// code running inside another framework's memory pool or arena (which must
+// see every byte it hands out), plug-ins loaded into a host that forbids
+// cudaMalloc/cudaFree on its threads, or real-time loops where an allocation
+// can stall.  They pass device inputs and outputs they already own; the only
+// other device memory this call touches is the fixed per-target key array
+// below, which the CUDA runtime reserves when the library's kernels are
+// loaded on a device and keeps until the process exits.
+namespace bmm {
+
+// Largest n_targets one call accepts: 16384 keys x 8 bytes = 128 KiB per device.
+constexpr size_t kNoAllocMaxTargets = 16384;
+
+static __device__ __align__(256) unsigned long long g_noalloc_keys[kNoAllocMaxTargets];
+
+namespace {
+struct NoAllocDevice {
+    bool ready = false;
+    unsigned long long* keys = nullptr;  // device address of g_noalloc_keys
+    int sm_count = 0;
+    int smem_optin = 0;
+};
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[kNoAllocMaxDevices];
+
+// Once per device, with that device current: resolve the array's device
+// address (a host-side reference to g_noalloc_keys is only a stand-in, never
+// a device address) and read the launch limits.  Allocates nothing.
+int noalloc_setup(NoAllocDevice** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return fail(BMM_ENODEV, "no CUDA device is available: %s", cudaGetErrorString(e));
+    if (dev < 0 || dev >= kNoAllocMaxDevices)
+        return fail(BMM_EINVAL, "gray targets (no-alloc): device %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    NoAllocDevice& d = g_noalloc_dev[dev];
+    if (!d.ready) {
+        void* addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_noalloc_keys);
+        if (e != cudaSuccess)
+            return fail(BMM_ECUDA, "cudaGetSymbolAddress(g_noalloc_keys) failed: %s",
+                        cudaGetErrorString(e));
+        int sms = 0, optin = 0;
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess)
+            e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e != cudaSuccess)
+            return fail(BMM_ECUDA, "device query failed: %s", cudaGetErrorString(e));
+        d.keys = static_cast<unsigned long long*>(addr);
+        d.sm_count = sms;
+        d.smem_optin = optin;
+        d.ready = true;
+    }
+    *out = &d;
+    return BMM_OK;
+}
+}  // namespace
+}  // namespace bmm
+
+extern "C" BMM_API int bmm_gray_targets_noalloc(const uint64_t* d_words, size_t rows, size_t stride,
+                                                size_t cols, const uint32_t* d_targets,
+                                                const uint32_t* d_others, size_t n_targets,
+                                                size_t k, int tiebreak, uint64_t* d_best_mask,
+                                                uint32_t* d_best_weight, void* stream) {
+    using namespace bmm;
+    clear_error();
+    (void)rows;
+    if (n_targets == 0)
+        return BMM_OK;
+    if (n_targets > kNoAllocMaxTargets)
+        return fail(BMM_EINVAL,
+                    "gray targets (no-alloc): %zu targets exceed the fixed scratch of %zu; split "
+                    "the call or use bmm_gray_targets_dev",
+                    n_targets, kNoAllocMaxTargets);
+    if (k < 1 || k > 40)
+        return fail(BMM_EINVAL, "gray targets (no-alloc): k must be in [1, 40]");
+    if (cols >= (1ull << 24))
+        return fail(BMM_EINVAL, "gray targets (no-alloc): cols must be < 2^24");
+    if ((cols + 63) / 64 > stride)
+        return fail(BMM_EINVAL, "gray targets (no-alloc): stride smaller than the row width");
+    if (!d_words || !d_targets || !d_others || !d_best_mask || !d_best_weight)
+        return fail(BMM_EINVAL, "gray targets (no-alloc): null argument");
+    NoAllocDevice* d = nullptr;
+    BMM_TRY(noalloc_setup(&d));
+    // Launch limits only; this Workspace owns no buffers and no stream.
+    Workspace limits;
+    limits.sm_count = d->sm_count;
+    limits.smem_optin = d->smem_optin;
+    const size_t W = (cols + 63) / 64;
+    int lanes = 1;
+    while ((size_t)lanes * 64 < W)
+        lanes *= 2;
+    int chunk = auto_chunk_bits((int)k, lanes, d->sm_count, (int)n_targets);
+    if (chunk > (int)k)
+        chunk = (int)k;
+    // gray_targets_launch clears the keys it uses to ~0 before the search, so
+    // whatever the previous call left in the array does not leak into this one.
+    return gray_targets_launch(&limits, d_words, (int)stride, (int)W, d_targets, d_others,
+                               (int)n_targets, (int)k, tiebreak, chunk, d->keys, d_best_mask,
+                               d_best_weight, (cudaStream_t)stream);
+}

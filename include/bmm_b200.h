@@ -143,6 +143,25 @@ BMM_API int bmm_gray_targets_dev(const uint64_t* d_words, size_t rows, size_t st
                          const uint32_t* d_targets, const uint32_t* d_others, size_t n_targets,
                          size_t k, int tiebreak, uint64_t* d_best_mask, uint32_t* d_best_weight,
                          void* stream);
+/* Allocation-free bmm_gray_targets_dev.  No counterpart in the reference.
+ * For callers that may not allocate device memory (a host framework's pool
+ * or arena that must account for every byte, plug-ins whose host forbids
+ * cudaMalloc/cudaFree, latency-critical loops): all pointers are device
+ * memory the caller owns, `stream` is a cudaStream_t, and the call runs
+ * asynchronously without cudaMalloc, cudaFree or any allocating routine.
+ * Its only scratch is a fixed per-device array of BMM_NOALLOC_MAX_TARGETS
+ * 64-bit keys (128 KiB) that exists on every device that loads this library
+ * until the process exits; n_targets above that limit is BMM_EINVAL.
+ * The first call on each device looks up that array's device address, so
+ * make the first call on a device before any stream capture.  All calls
+ * share the array: calls whose executions overlap on the GPU (different
+ * streams, or different host threads) race; serialise them. */
+#define BMM_NOALLOC_MAX_TARGETS 16384
+BMM_API int bmm_gray_targets_noalloc(const uint64_t* d_words, size_t rows, size_t stride,
+                                     size_t cols, const uint32_t* d_targets,
+                                     const uint32_t* d_others, size_t n_targets, size_t k,
+                                     int tiebreak, uint64_t* d_best_mask,
+                                     uint32_t* d_best_weight, void* stream);
 BMM_API int bmm_fwht_targets(const uint64_t* words, size_t rows, size_t stride, size_t cols,
                      const uint32_t* targets, const uint32_t* others, size_t n_targets, size_t k,
                      uint64_t* best_mask, uint32_t* best_weight);
