@@ -44,6 +44,7 @@ _candp = C.POINTER(Candidate_t)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
     "bmm_probe_xor_popc": [C.POINTER(C.c_double)],
+    "bmm_gray_tune": [C.c_int, C.c_int],
     "bmm_last_error": [],
     "bmm_version": [],
     "bmm_runtime_features": [C.POINTER(Features_t)],
@@ -51,6 +52,7 @@ SIGNATURES = {
     "bmm_fwht_i16": [_i16p, _sz],
     "bmm_fwht_i32_dev": [_vp, _sz, _vp],
     "bmm_fwht_search": [_u64p, _sz, _sz, _u32p, _sz, _sz, _sz, _candp, _szp],
+    "bmm_mitm_search": [_u64p, _sz, _sz, _u32p, _sz, _sz, _sz, _candp, _szp],
     "bmm_gray_search": [_u64p, _sz, _sz, _u32p, _sz, _sz, _sz, _candp, _szp],
     "bmm_gray_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, C.c_int, _u64p, _u32p],
     "bmm_gray_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, C.c_int, _vp, _vp, _vp],

@@ -4,6 +4,7 @@
 #include "common.cuh"
 #include "fwht.cuh"
 #include "gray.cuh"
+#include "spectrum.cuh"
 #include "topk.cuh"
 
 #include <cstdio>
@@ -226,7 +227,10 @@ int fwht_host(T* data, size_t n) {
         return st;
     void* d = nullptr;
     BMM_TRY(upload(ws, kSlotSpec, data, n * sizeof(T), &d));
-    BMM_TRY(fwht_global_launch<T>(ws, (T*)d, t, ws->stream));
+    if (sizeof(T) == 4 && t >= 14)
+        BMM_TRY(spectrum_dense_fwht(ws, (int32_t*)d, t, ws->stream));
+    else
+        BMM_TRY(fwht_global_launch<T>(ws, (T*)d, t, ws->stream));
     BMM_CUDA_TRY(cudaMemcpyAsync(data, d, n * sizeof(T), cudaMemcpyDeviceToHost, ws->stream));
     BMM_CUDA_TRY(cudaStreamSynchronize(ws->stream));
     return BMM_OK;
@@ -267,6 +271,17 @@ uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stri
             words[i * stride + w] ^= words[j * stride + w];
     }
     return planted;
+}
+
+int bmm_gray_tune(int hs_blocks, int chunk_bits) {
+    clear_error();
+    if (hs_blocks < -1 || hs_blocks > 8 || hs_blocks == 1 || hs_blocks == 7)
+        return fail(BMM_EINVAL, "gray tuning: hs_blocks must be -1, 0, 2-6 or 8");
+    if (chunk_bits < -1 || chunk_bits > 31)
+        return fail(BMM_EINVAL, "gray tuning: chunk_bits must be -1 or in [0, 31]");
+    g_gray_tuning.hs_blocks = hs_blocks;
+    g_gray_tuning.chunk_bits = chunk_bits;
+    return BMM_OK;
 }
 
 int bmm_probe_xor_popc(double* words_per_second) {
@@ -316,6 +331,8 @@ int bmm_fwht_i32_dev(int32_t* d_data, size_t n, void* stream) {
     Workspace* ws = workspace(&st);
     if (!ws)
         return st;
+    if (t >= 14)
+        return spectrum_dense_fwht(ws, d_data, t, (cudaStream_t)stream);
     return fwht_global_launch<int32_t>(ws, d_data, t, (cudaStream_t)stream);
 }
 
@@ -331,13 +348,15 @@ int bmm_fwht_search(const uint64_t* words, size_t stride, size_t cols, const uin
         return BMM_OK;
     if (t > 64)
         return fail(BMM_EINVAL, "FwhtSearch: window_rows size must be <= 64");
-    if (t > 30)
-        return fail(BMM_EINVAL, "FwhtSearch: window_rows size %zu exceeds the 2^30-bucket device "
+    if (t > 33)
+        return fail(BMM_EINVAL, "FwhtSearch: window_rows size %zu exceeds the 2^33-bucket device "
                                 "spectrum limit", t);
     BMM_TRY(check_window(words, stride, cols, win, t, "FwhtSearch"));
     const size_t W = (cols + 63) / 64;
     if (W == 0)
         return BMM_OK;
+    if (cols > 0x7fffffffull)
+        return fail(BMM_EOVERFLOW, "FwhtSearch: total weight exceeds int32 range");
     const size_t n = (size_t)1 << t;
     size_t kk = k < n - 1 ? k : n - 1;
     if (kk > 1024)
@@ -348,22 +367,51 @@ int bmm_fwht_search(const uint64_t* words, size_t stride, size_t cols, const uin
     if (!ws)
         return st;
     const std::vector<uint64_t> packed = pack_window(words, stride, W, win, t);
-    void *d_rows = nullptr, *d_spec = nullptr, *d_total = nullptr, *d_out = nullptr;
+    void *d_rows = nullptr, *d_out = nullptr;
     BMM_TRY(upload(ws, kSlotRows, packed.data(), packed.size() * 8, &d_rows));
-    BMM_TRY(ws_buffer(ws, kSlotSpec, n * sizeof(int32_t), &d_spec));
-    BMM_TRY(ws_buffer(ws, kSlotCounter, 16, &d_total));
     BMM_TRY(ws_buffer(ws, kSlotOut, kk * sizeof(bmm_candidate), &d_out));
-    BMM_TRY(fwht_window_search_launch(ws, (const uint64_t*)d_rows, (int)t, (int)W, (long long)cols,
-                                      (int)kk, (int32_t*)d_spec, (unsigned long long*)d_total,
-                                      (bmm_candidate*)d_out, ws->stream));
-    unsigned long long total = 0;
-    BMM_CUDA_TRY(cudaMemcpyAsync(&total, d_total, 8, cudaMemcpyDeviceToHost, ws->stream));
-    BMM_TRY(finish_candidates(ws, (bmm_candidate*)d_out, kk, out, out_count));
-    if (total > 0x7fffffffull) {  // fwht_search.cpp:77-87
-        *out_count = 0;
-        return fail(BMM_EOVERFLOW, "FwhtSearch: total weight exceeds int32 range");
-    }
-    return BMM_OK;
+    BMM_TRY(spectrum_topk_launch(ws, (const uint64_t*)d_rows, (int)t, (int)W, (long long)cols,
+                                 (int)kk, (bmm_candidate*)d_out, ws->stream));
+    return finish_candidates(ws, (bmm_candidate*)d_out, kk, out, out_count);
+}
+
+int bmm_mitm_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
+                    size_t t, size_t k, size_t low_bits, bmm_candidate* out, size_t* out_count) {
+    clear_error();
+    if (!out_count)
+        return fail(BMM_EINVAL, "MitmFwhtSearch: null out_count");
+    *out_count = 0;
+    // src/search/mitm_fwht_search.cpp:270-289
+    if (k == 0 || t == 0)
+        return BMM_OK;
+    if (t > 64)
+        return fail(BMM_EINVAL, "MitmFwhtSearch: window_rows size must be <= 64");
+    if (t > 40)
+        return fail(BMM_EINVAL, "MitmFwhtSearch: 2^%zu combinations cannot be enumerated", t);
+    if (low_bits != 0 && low_bits >= t)
+        return fail(BMM_EINVAL, "MitmFwhtSearch: low_bits must be in [1, t - 1] or 0 for auto");
+    BMM_TRY(check_window(words, stride, cols, win, t, "MitmFwhtSearch"));
+    const size_t W = (cols + 63) / 64;
+    if (W == 0)
+        return BMM_OK;
+    if (cols > 0x7fffffffull)
+        return fail(BMM_EOVERFLOW, "build_compact_split_window: total weight exceeds int32 range");
+    const size_t states = ((size_t)1 << t) - 1;
+    const size_t kk = k < states ? k : states;
+    if (kk > 1024)
+        return fail(BMM_EINVAL, "MitmFwhtSearch: max_candidates above 1024 is not supported on "
+                                "the device (requested %zu)", k);
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    const std::vector<uint64_t> packed = pack_window(words, stride, W, win, t);
+    void *d_rows = nullptr, *d_out = nullptr;
+    BMM_TRY(upload(ws, kSlotRows, packed.data(), packed.size() * 8, &d_rows));
+    BMM_TRY(ws_buffer(ws, kSlotOut, kk * sizeof(bmm_candidate), &d_out));
+    BMM_TRY(spectrum_topk_launch(ws, (const uint64_t*)d_rows, (int)t, (int)W, (long long)cols,
+                                 (int)kk, (bmm_candidate*)d_out, ws->stream));
+    return finish_candidates(ws, (bmm_candidate*)d_out, kk, out, out_count);
 }
 
 int bmm_gray_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
@@ -456,6 +504,8 @@ static int gray_targets_common(Workspace* ws, const uint64_t* d_words, size_t ro
         lanes = (int)G;
     }
     int chunk = auto_chunk_bits((int)k, lanes, ws->sm_count, (int)n_targets);
+    if (g_gray_tuning.chunk_bits > 0)
+        chunk = g_gray_tuning.chunk_bits;
     if (chunk > (int)k)
         chunk = (int)k;
     void* d_keys = nullptr;

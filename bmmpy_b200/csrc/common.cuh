@@ -46,6 +46,7 @@ enum Slot : int {
     kSlotCounter,
     kSlotExtra0,
     kSlotExtra1,
+    kSlotSlices,
     kSlotCount
 };
 

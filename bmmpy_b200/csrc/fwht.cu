@@ -9,12 +9,10 @@
 //    exact top-k by (weight, mask) over masks >= 1.
 //
 // B200 design:
-//  * Large spectra live in HBM and are transformed in passes; each pass moves
-//    one 2^(r+b)-element tile (r stage bits x 2^b consecutive low elements so
-//    loads stay in whole 32-byte sectors) through shared memory and applies r
-//    stages there.  A spectrum of 2^t int32 costs ceil(t / r) read+write
-//    sweeps -- this is the HBM-bound path.
-//  * The last sweep is followed by a fused weight + warp-register top-k scan.
+//  * Small transforms (and all int16 ones) move one 2^(r+b)-element tile
+//    (r stage bits x 2^b consecutive low elements) through shared memory per
+//    pass; int32 transforms of 2^14 elements and more use the register-round
+//    passes of spectrum.cu.
 //  * Per-target searches (t <= 16 others, cols <= 32767) never touch HBM: the
 //    whole spectrum stays in shared memory and registers of one CTA, with two
 //    int16 half-spectra packed into each int32 (h[i] + 65536*h[i + n/2]); the
@@ -67,74 +65,6 @@ __global__ void __launch_bounds__(256)
             d[base + ((unsigned long long)j << lo) + i] = s[e];
         }
         __syncthreads();
-    }
-}
-
-// Column-pattern histogram of the active columns of t window rows (t x W
-// words, packed).  spec[p] += 1 for every column whose pattern p != 0.
-__global__ void hist_kernel(const uint64_t* __restrict__ rows, int t, int W, long long cols,
-                            int32_t* __restrict__ spec, unsigned long long* __restrict__ total) {
-    unsigned long long local = 0;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < cols;
-         c += (long long)gridDim.x * blockDim.x) {
-        const long long w = c >> 6;
-        const int bit = (int)(c & 63);
-        uint32_t p = 0;
-        for (int r = 0; r < t; ++r)
-            p |= (uint32_t)((__ldg(rows + (size_t)r * W + w) >> bit) & 1ull) << r;
-        if (p) {
-            atomicAdd(spec + p, 1);
-            ++local;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-        local += __shfl_xor_sync(kFull, local, o);
-    if ((threadIdx.x & 31) == 0 && local)
-        atomicAdd(total, local);
-}
-
-// Weight + top-kk scan over masks 1..2^t-1 of a transformed spectrum.
-template <int E>
-__global__ void __launch_bounds__(256)
-    scan_topk_kernel(const int32_t* __restrict__ spec, int t,
-                     const unsigned long long* __restrict__ total, int kk,
-                     bmm_candidate* __restrict__ cta_out) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    bmm_candidate* stage = reinterpret_cast<bmm_candidate*>(smem_raw);
-    const long long n = 1ll << t;
-    const long long N = (long long)*total;
-    WarpTopK<E> top;
-    top.init();
-    uint32_t thr = 0xffffffffu;
-    const long long start = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long step = (long long)gridDim.x * blockDim.x;
-    // warp-uniform trip count
-    const long long base0 = start - (threadIdx.x & 31);
-    for (long long b0 = base0; b0 < n; b0 += step) {
-        const long long m = b0 + (threadIdx.x & 31);
-        bool ok = m >= 1 && m < n;
-        uint32_t w = 0xffffffffu;
-        if (ok) {
-            const long long w2 = N - (long long)spec[m];
-            ok = w2 >= 0 && (w2 & 1) == 0;
-            w = (uint32_t)(w2 >> 1);
-        }
-        top.offer(ok, w, (uint64_t)m, kk, thr);
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    top.store(stage + warp * 32 * E, 32 * E);
-    __syncthreads();
-    if (warp == 0) {
-        for (int ow = 1; ow < (int)(blockDim.x >> 5); ++ow)
-            for (int base = 0; base < 32 * E; base += 32) {
-                const bmm_candidate c = stage[ow * 32 * E + base + lane];
-                const bool ok = c.weight != 0xffffffffu;
-                if (!__any_sync(kFull, ok && c.weight <= thr))
-                    break;
-                top.offer(ok, c.weight, c.mask, kk, thr);
-            }
-        top.store(cta_out + (size_t)blockIdx.x * kk, kk);
     }
 }
 
@@ -367,47 +297,6 @@ int fwht_global_launch(Workspace* ws, T* d, int t, cudaStream_t stream) {
 
 template int fwht_global_launch<int32_t>(Workspace*, int32_t*, int, cudaStream_t);
 template int fwht_global_launch<int16_t>(Workspace*, int16_t*, int, cudaStream_t);
-
-int fwht_window_search_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, long long cols,
-                              int kk, int32_t* d_spec, unsigned long long* d_total,
-                              bmm_candidate* d_out, cudaStream_t stream) {
-    const size_t n = (size_t)1 << t;
-    BMM_CUDA_TRY(cudaMemsetAsync(d_spec, 0, n * sizeof(int32_t), stream));
-    BMM_CUDA_TRY(cudaMemsetAsync(d_total, 0, sizeof(unsigned long long), stream));
-    {
-        long long blocks = (cols + 255) / 256;
-        if (blocks > (long long)ws->sm_count * 8)
-            blocks = (long long)ws->sm_count * 8;
-        if (blocks < 1)
-            blocks = 1;
-        hist_kernel<<<(unsigned)blocks, 256, 0, stream>>>(d_rows, t, W, cols, d_spec, d_total);
-        BMM_CUDA_TRY(cudaGetLastError());
-    }
-    BMM_TRY(fwht_global_launch<int32_t>(ws, d_spec, t, stream));
-    auto run = [&](auto Ec) -> int {
-        constexpr int E = decltype(Ec)::value;
-        auto kern = scan_topk_kernel<E>;
-        const size_t smem = (size_t)8 * 32 * E * sizeof(bmm_candidate);
-        BMM_CUDA_TRY(
-            cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        long long blocks = ((long long)n + 255) / 256;
-        if (blocks > (long long)ws->sm_count * 4)
-            blocks = (long long)ws->sm_count * 4;
-        bmm_candidate* lists = nullptr;
-        BMM_TRY(ws_buffer(ws, kSlotCand, (size_t)blocks * kk * sizeof(bmm_candidate),
-                          (void**)&lists));
-        kern<<<(unsigned)blocks, 256, smem, stream>>>(d_spec, t, d_total, kk, lists);
-        BMM_CUDA_TRY(cudaGetLastError());
-        return merge_topk_lists(lists, (int)blocks, kk, d_out, stream);
-    };
-    if (kk <= 32)
-        return run(std::integral_constant<int, 1>{});
-    if (kk <= 128)
-        return run(std::integral_constant<int, 4>{});
-    if (kk <= 1024)
-        return run(std::integral_constant<int, 32>{});
-    return fail(BMM_EINVAL, "fwht search: k must be <= 1024");
-}
 
 int fwht_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int cols,
                         const uint32_t* d_targets, const uint32_t* d_others, int n_items, int k,

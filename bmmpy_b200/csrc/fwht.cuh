@@ -9,13 +9,6 @@ namespace bmm {
 template <typename T>
 int fwht_global_launch(Workspace* ws, T* d, int t, cudaStream_t stream);
 
-// FwhtSearch over t window rows packed in d_rows (t x W words): histogram into
-// d_spec (2^t int32), transform, scan; d_total receives the active column
-// count; d_out receives kk candidates.
-int fwht_window_search_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, long long cols,
-                              int kk, int32_t* d_spec, unsigned long long* d_total,
-                              bmm_candidate* d_out, cudaStream_t stream);
-
 // Per-target best for n_items (target, k others) items; k <= 16, cols <= 32767.
 int fwht_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int cols,
                         const uint32_t* d_targets, const uint32_t* d_others, int n_items, int k,

@@ -40,6 +40,76 @@ __device__ __forceinline__ uint32_t xor_row_popc(uint64_t (&cur)[WPL], const uin
     return s;
 }
 
+// Carry-save adder: l = a ^ b ^ c (weight 1), h = majority(a, b, c) (weight 2).
+__device__ __forceinline__ void csa(uint32_t& h, uint32_t& l, uint32_t a, uint32_t b, uint32_t c) {
+    const uint32_t u = a ^ b;
+    h = (a & b) | (u & c);
+    l = u ^ c;
+}
+
+// Harley-Seal step over 16 words (Mula, Kurz, Lemire, "Faster population
+// counts using AVX2 instructions", 2018): 15 carry-save adders fold the block
+// into running ones/twos/fours/eights and emit one "sixteens" word, so 16
+// words cost 30 LOP3 + 1 POPC instead of 16 POPC.
+__device__ __forceinline__ void hs16(const uint32_t (&d)[16], uint32_t& ones, uint32_t& twos,
+                                     uint32_t& fours, uint32_t& eights, uint32_t& n16) {
+    uint32_t twosA, twosB, foursA, foursB, eightsA, eightsB, sixteens;
+    csa(twosA, ones, ones, d[0], d[1]);
+    csa(twosB, ones, ones, d[2], d[3]);
+    csa(foursA, twos, twos, twosA, twosB);
+    csa(twosA, ones, ones, d[4], d[5]);
+    csa(twosB, ones, ones, d[6], d[7]);
+    csa(foursB, twos, twos, twosA, twosB);
+    csa(eightsA, fours, fours, foursA, foursB);
+    csa(twosA, ones, ones, d[8], d[9]);
+    csa(twosB, ones, ones, d[10], d[11]);
+    csa(foursA, twos, twos, twosA, twosB);
+    csa(twosA, ones, ones, d[12], d[13]);
+    csa(twosB, ones, ones, d[14], d[15]);
+    csa(foursB, twos, twos, twosA, twosB);
+    csa(eightsB, fours, fours, foursA, foursB);
+    csa(sixteens, eights, eights, eightsA, eightsB);
+    n16 += __popc(sixteens);
+}
+
+// XOR a shared-memory row into cur and return popcount(cur).  The first
+// NHB blocks of 8 words go through the carry-save tree (ALU pipe), the rest
+// through POPC (XU pipe); NHB balances the two pipes.
+template <int WPL, int NHB>
+__device__ __forceinline__ uint32_t xor_row_popc_hs(uint64_t (&cur)[WPL], const uint64_t* srow) {
+    static_assert(NHB * 8 <= WPL, "carry-save blocks exceed the row");
+    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(srow);
+    uint32_t ones = 0, twos = 0, fours = 0, eights = 0, n16 = 0;
+#pragma unroll
+    for (int blk = 0; blk < NHB; ++blk) {
+        uint32_t d[16];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const ulonglong2 v = p[blk * 4 + j];
+            uint64_t& a = cur[blk * 8 + 2 * j];
+            uint64_t& b = cur[blk * 8 + 2 * j + 1];
+            a ^= v.x;
+            b ^= v.y;
+            d[4 * j + 0] = (uint32_t)a;
+            d[4 * j + 1] = (uint32_t)(a >> 32);
+            d[4 * j + 2] = (uint32_t)b;
+            d[4 * j + 3] = (uint32_t)(b >> 32);
+        }
+        hs16(d, ones, twos, fours, eights, n16);
+    }
+    uint32_t s = 0;
+#pragma unroll
+    for (int i = NHB * 4; i < WPL / 2; ++i) {
+        const ulonglong2 v = p[i];
+        cur[2 * i] ^= v.x;
+        cur[2 * i + 1] ^= v.y;
+        s += __popcll(cur[2 * i]) + __popcll(cur[2 * i + 1]);
+    }
+    if (NHB > 0)
+        s += 16 * n16 + 8 * __popc(eights) + 4 * __popc(fours) + 2 * __popc(twos) + __popc(ones);
+    return s;
+}
+
 template <int WPL>
 __device__ __forceinline__ void xor_row(uint64_t (&cur)[WPL], const uint64_t* srow) {
     const ulonglong2* p = reinterpret_cast<const ulonglong2*>(srow);
@@ -82,7 +152,7 @@ __device__ __forceinline__ void stage_rows(uint64_t* srow, int nrows, int W, Row
 // ---------------------------------------------------------------------------
 // Window search: top-kk over all nonzero masks of t rows.
 // rows: t x W words (device, packed in window order).
-template <int WPL, int G, int E>
+template <int WPL, int G, int E, int NHB>
 __global__ void __launch_bounds__(kThreads)
     gray_window_kernel(const uint64_t* __restrict__ rows, int t, int W, int chunk,
                        unsigned long long n_prefix, int kk, bmm_candidate* __restrict__ cta_out) {
@@ -118,7 +188,7 @@ __global__ void __launch_bounds__(kThreads)
         top.offer(valid && mask != 0, w, mask, kk, thr);
         for (uint32_t s = 1; s < states; ++s) {
             const int b = __ffs(s) - 1;
-            w = group_sum<G>(xor_row_popc<WPL>(cur, my + (size_t)b * SW));
+            w = group_sum<G>(xor_row_popc_hs<WPL, NHB>(cur, my + (size_t)b * SW));
             mask ^= 1ull << b;
             top.offer(valid, w, mask, kk, thr);
         }
@@ -148,7 +218,7 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------
 // Per-target top-1.  CTA b serves target b / ctas_per_target.
 // key = (weight << 40) | tie, tie = S (tiebreak 0) or inverse-Gray(S).
-template <int WPL, int G>
+template <int WPL, int G, int NHB>
 __global__ void __launch_bounds__(kThreads)
     gray_targets_kernel(const uint64_t* __restrict__ words, int stride, int W,
                         const uint32_t* __restrict__ targets, const uint32_t* __restrict__ others,
@@ -200,7 +270,7 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t states = 1u << chunk;
     for (uint32_t s = 1; s < states; ++s) {
         const int b = __ffs(s) - 1;
-        const uint32_t w = group_sum<G>(xor_row_popc<WPL>(cur, my + (size_t)b * SW));
+        const uint32_t w = group_sum<G>(xor_row_popc_hs<WPL, NHB>(cur, my + (size_t)b * SW));
         low ^= 1ull << b;
         if (w <= best_w) {
             const uint64_t tie = tiebreak ? (hi_tie | (s ^ flip)) : (hi_mask | low);
@@ -236,6 +306,13 @@ __global__ void decode_keys_kernel(const unsigned long long* __restrict__ keys, 
 
 // ---------------------------------------------------------------------------
 // host side
+
+// Carry-save blocks (of 8 words) per Gray step by lane width.  Without them
+// the XU pipe (POPC) saturates while ALU idles at ~36 %; 5 of the 8 blocks of
+// a 64-word lane through the adder tree measured fastest on B200 (40 x 4096,
+// k = 24: 20.3 ms -> 15.7 ms per step); narrower lanes keep the same ratio.
+constexpr int default_nhb(int wpl) { return wpl >= 64 ? 5 : wpl >= 32 ? 2 : wpl >= 16 ? 1 : 0; }
+
 int group_shape(size_t W, int* wpl, int* g) {
     if (W <= 2) {
         *wpl = 2, *g = 1;
@@ -293,16 +370,21 @@ int dispatch_e(int kk, F&& f) {
 
 }  // namespace
 
+GrayTuning g_gray_tuning;
+
 int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items) {
-    // enough prefixes for ~8 resident CTAs of 128 threads per SM, with at
-    // least 2^6 Gray steps per prefix
-    const double want = (double)sm_count * 8 * kThreads / lanes_per_prefix / (n_items ? n_items : 1);
+    // Enough independent prefixes for ~32 waves of 128-thread CTAs at 3 CTAs
+    // per SM (so the last wave's tail is small), but keep at least 2^8 Gray
+    // steps per prefix so the prefix set-up (up to t - chunk row XORs) stays
+    // cheap.  Measured on 40 x 4096, k = 24: chunk 10 beats 12 by 9 %.
+    const double want =
+        (double)sm_count * 3 * 32 * kThreads / lanes_per_prefix / (n_items ? n_items : 1);
     int hb = 0;
     while (hb < t && (double)(1ull << hb) < want)
         ++hb;
     int chunk = t - hb;
-    if (chunk < 6)
-        chunk = t < 6 ? t : 6;
+    if (chunk < 8)
+        chunk = t < 8 ? t : 8;
     if (chunk > 20)
         chunk = 20;
     if (chunk > t)
@@ -320,7 +402,7 @@ int gray_window_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, int 
         constexpr int WPL = decltype(WPLc)::value, G = decltype(Gc)::value;
         return dispatch_e(kk, [&](auto Ec) -> int {
             constexpr int E = decltype(Ec)::value;
-            auto kern = gray_window_kernel<WPL, G, E>;
+            auto kern = gray_window_kernel<WPL, G, E, default_nhb(WPL)>;
             const size_t merge_bytes = (size_t)(kThreads / 32) * 32 * E * sizeof(bmm_candidate);
             const size_t smem = srow_bytes > merge_bytes ? srow_bytes : merge_bytes;
             if (smem > (size_t)ws->smem_optin)
@@ -365,13 +447,30 @@ int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int 
     BMM_CUDA_TRY(cudaMemsetAsync(d_keys, 0xff, sizeof(unsigned long long) * n_targets, stream));
     BMM_TRY(dispatch_wg(wpl, g, [&](auto WPLc, auto Gc) -> int {
         constexpr int WPL = decltype(WPLc)::value, G = decltype(Gc)::value;
-        auto kern = gray_targets_kernel<WPL, G>;
-        BMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
-        kern<<<(unsigned)(ctas * n_targets), kThreads, smem, stream>>>(
-            d_words, stride, W, d_targets, d_others, k, chunk, tiebreak, (int)ctas, d_keys);
-        BMM_CUDA_TRY(cudaGetLastError());
-        return BMM_OK;
+        auto go = [&](auto kern) -> int {
+            BMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)smem));
+            kern<<<(unsigned)(ctas * n_targets), kThreads, smem, stream>>>(
+                d_words, stride, W, d_targets, d_others, k, chunk, tiebreak, (int)ctas, d_keys);
+            BMM_CUDA_TRY(cudaGetLastError());
+            return BMM_OK;
+        };
+        const int hs = g_gray_tuning.hs_blocks;
+        if constexpr (WPL == 64 && G == 1) {
+            switch (hs) {
+            case -1: break;
+            case 0: return go(gray_targets_kernel<WPL, G, 0>);
+            case 2: return go(gray_targets_kernel<WPL, G, 2>);
+            case 3: return go(gray_targets_kernel<WPL, G, 3>);
+            case 4: return go(gray_targets_kernel<WPL, G, 4>);
+            case 5: return go(gray_targets_kernel<WPL, G, 5>);
+            case 6: return go(gray_targets_kernel<WPL, G, 6>);
+            case 8: return go(gray_targets_kernel<WPL, G, 8>);
+            default: return fail(BMM_EINVAL, "gray tuning: hs_blocks must be 0, 2-6 or 8");
+            }
+        }
+        (void)hs;
+        return go(gray_targets_kernel<WPL, G, default_nhb(WPL)>);
     }));
     decode_keys_kernel<<<(n_targets + 127) / 128, 128, 0, stream>>>(d_keys, n_targets, tiebreak,
                                                                     d_best_mask, d_best_weight);

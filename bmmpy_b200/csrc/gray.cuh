@@ -6,6 +6,13 @@
 
 namespace bmm {
 
+// Overrides used by the autotuner; -1 selects the built-in policy.
+struct GrayTuning {
+    int hs_blocks = -1;   // carry-save blocks per 64-word lane (0, 2-6, 8)
+    int chunk_bits = -1;  // Gray-swept low bits per prefix
+};
+extern GrayTuning g_gray_tuning;
+
 // Low chunk width giving enough independent prefixes to fill the device.
 int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items);
 

@@ -1,0 +1,568 @@
+// Exact top-k over the full Walsh-Hadamard spectrum of a window, in HBM.
+//
+// Serves FwhtSearch (src/search/fwht_search.cpp:34-132) and MitmFwhtSearch
+// (src/search/mitm_fwht_search.cpp:267-322): both return the k smallest
+// (weight, mask) over all nonzero masks of the t window rows, with
+// weight(mask) = (N - WHT[mask]) / 2, N = active columns and WHT the
+// transform of the active columns' t-bit pattern histogram.
+//
+// B200 design.  The 2^T spectrum (T = min(t, 33); 2^33 int32 = 32 GB) lives in
+// HBM and is produced in tiled passes of 2^14 int32 (64 KB of shared memory,
+// 256 threads, 64 values per thread, stages applied in register rounds of up
+// to six bits over a bank-swizzled tile):
+//   pass A (bits 0..13): each tile is BUILT from the columns whose pattern
+//       falls in it (columns bucketed by tile with a counting sort), so the
+//       sparse histogram is never written; empty tiles are written as zeros;
+//   middle passes (<= 9 bits, 32 consecutive elements per row so every warp
+//       access is a full 128-byte line): read, transform, write;
+//   the last pass keeps its values in registers and feeds the weight + top-k
+//       scan instead of writing (warp-register top-k lists, merged at the end).
+// For t > 33 the extra high bits are enumerated (meet-in-the-middle): slice x
+// transforms the low 33 bits of the histogram signed by parity(high & x).
+// Traffic for t = 32: write 16 GB + read/write 32 GB + read 16 GB.
+#include "common.cuh"
+#include "spectrum.cuh"
+#include "topk.cuh"
+
+namespace bmm {
+namespace {
+
+constexpr int kTileLog = 14;
+constexpr int kTile = 1 << kTileLog;
+constexpr int kThr = 256;
+constexpr int kPer = kTile / kThr;  // 64
+static_assert(kPer == 64, "register rounds assume 64 values per thread");
+
+__device__ __forceinline__ int swz(int k) { return k ^ ((k >> 6) & 31); }
+
+// One register round: the thread holds the 64 tile elements
+// k = base(tid) | (e << WL), e in [0, 64), and applies the stages on e bits
+// [S0, S0 + NS).  base places tid's 8 bits outside [WL, WL + 6).
+template <int WL>
+__device__ __forceinline__ int round_base(int tid) {
+    return ((tid >> WL) << (WL + 6)) | (tid & ((1 << WL) - 1));
+}
+
+template <int S0, int NS>
+__device__ __forceinline__ void bfly(int32_t (&x)[64]) {
+#pragma unroll
+    for (int s = S0; s < S0 + NS; ++s) {
+#pragma unroll
+        for (int e = 0; e < 64; ++e)
+            if ((e & (1 << s)) == 0) {
+                const uint32_t u = (uint32_t)x[e], v = (uint32_t)x[e | (1 << s)];
+                x[e] = (int32_t)(u + v);
+                x[e | (1 << s)] = (int32_t)(u - v);
+            }
+    }
+}
+
+template <int WL, int S0, int NS>
+__device__ __forceinline__ void round_load(const int32_t* s, int32_t (&x)[64]) {
+    const int base = round_base<WL>(threadIdx.x);
+#pragma unroll
+    for (int e = 0; e < 64; ++e)
+        x[e] = s[swz(base | (e << WL))];
+    bfly<S0, NS>(x);
+}
+
+template <int WL>
+__device__ __forceinline__ void round_store(int32_t* s, const int32_t (&x)[64]) {
+    const int base = round_base<WL>(threadIdx.x);
+#pragma unroll
+    for (int e = 0; e < 64; ++e)
+        s[swz(base | (e << WL))] = x[e];
+}
+
+// Offer the 64 register values of the last round to the warp's top-k.
+// Global mask of element k of the tile: mask_of(k).
+template <int WL, int E, typename MaskOf>
+__device__ __forceinline__ void scan_values(const int32_t (&x)[64], long long N, int kk,
+                                            WarpTopK<E>& top, uint32_t& thr, MaskOf mask_of) {
+    const int base = round_base<WL>(threadIdx.x);
+#pragma unroll
+    for (int e = 0; e < 64; ++e) {
+        const uint64_t mask = mask_of(base | (e << WL));
+        const long long w2 = N - (long long)x[e];
+        const bool ok = mask != 0 && w2 >= 0 && (w2 & 1) == 0;
+        top.offer(ok, (uint32_t)(w2 >> 1), mask, kk, thr);
+    }
+}
+
+template <int E>
+__device__ __forceinline__ void cta_list_out(WarpTopK<E>& top, uint32_t& thr, int kk,
+                                             bmm_candidate* stage, bmm_candidate* out) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __syncthreads();
+    top.store(stage + warp * 32 * E, 32 * E);
+    __syncthreads();
+    if (warp == 0) {
+        for (int ow = 1; ow < kThr / 32; ++ow)
+            for (int base = 0; base < 32 * E; base += 32) {
+                const bmm_candidate c = stage[ow * 32 * E + base + lane];
+                const bool ok = c.weight != 0xffffffffu;
+                if (!__any_sync(kFull, ok && c.weight <= thr))
+                    break;
+                top.offer(ok, c.weight, c.mask, kk, thr);
+            }
+        top.store(out, kk);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Column patterns of the active columns (pattern != 0) of t rows (t x W words).
+__global__ void patterns_kernel(const uint64_t* __restrict__ rows, int t, int W, long long cols,
+                                uint64_t* __restrict__ pats, unsigned long long* __restrict__ count) {
+    const int lane = threadIdx.x & 31;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c0 = blockIdx.x * (long long)blockDim.x + (threadIdx.x & ~31); c0 < cols;
+         c0 += stride) {
+        const long long c = c0 + lane;
+        uint64_t p = 0;
+        if (c < cols) {
+            const long long w = c >> 6;
+            const int bit = (int)(c & 63);
+            for (int r = 0; r < t; ++r)
+                p |= ((__ldg(rows + (size_t)r * W + w) >> bit) & 1ull) << r;
+        }
+        // one atomic per warp for the active columns it found
+        const unsigned bal = __ballot_sync(kFull, p != 0);
+        if (bal) {
+            unsigned long long base = 0;
+            if (lane == 0)
+                base = atomicAdd(count, (unsigned long long)__popc(bal));
+            base = __shfl_sync(kFull, base, 0);
+            if (p)
+                pats[base + __popc(bal & ((1u << lane) - 1))] = p;
+        }
+    }
+}
+
+// Counting sort of the patterns by pass-A tile: (p & lowmask) >> 14.
+__global__ void tile_count_kernel(const uint64_t* __restrict__ pats,
+                                  const unsigned long long* __restrict__ count, int T,
+                                  unsigned* __restrict__ counts) {
+    const unsigned long long n = *count;
+    const uint64_t lowmask = T >= 64 ? ~0ull : ((1ull << T) - 1);
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        atomicAdd(counts + ((pats[i] & lowmask) >> kTileLog), 1u);
+}
+
+// Exclusive scan of n counts (one CTA of 1024 threads); offsets has n + 1
+// entries; cursor receives a copy of the first n offsets.
+__global__ void __launch_bounds__(1024) exclusive_scan_kernel(const unsigned* __restrict__ counts,
+                                                              long long n,
+                                                              unsigned* __restrict__ offsets,
+                                                              unsigned* __restrict__ cursor) {
+    __shared__ unsigned sums[1024];
+    const long long per = (n + 1023) / 1024;
+    const long long lo = threadIdx.x * per;
+    const long long hi = lo + per < n ? lo + per : n;
+    unsigned s = 0;
+    for (long long i = lo; i < hi; ++i)
+        s += counts[i];
+    sums[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const unsigned v = threadIdx.x >= (unsigned)off ? sums[threadIdx.x - off] : 0u;
+        __syncthreads();
+        sums[threadIdx.x] += v;
+        __syncthreads();
+    }
+    unsigned run = threadIdx.x ? sums[threadIdx.x - 1] : 0u;
+    for (long long i = lo; i < hi; ++i) {
+        offsets[i] = run;
+        cursor[i] = run;
+        run += counts[i];
+    }
+    if (threadIdx.x == 1023)
+        offsets[n] = sums[1023];
+}
+
+__global__ void tile_scatter_kernel(const uint64_t* __restrict__ pats,
+                                    const unsigned long long* __restrict__ count, int T,
+                                    unsigned* __restrict__ cursor, uint64_t* __restrict__ sorted) {
+    const unsigned long long n = *count;
+    const uint64_t lowmask = T >= 64 ? ~0ull : ((1ull << T) - 1);
+    for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const uint64_t p = pats[i];
+        const unsigned pos = atomicAdd(cursor + ((p & lowmask) >> kTileLog), 1u);
+        sorted[pos] = p;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Pass A: bits 0..13.  SPARSE: tile built from its bucketed patterns (value
+// (-1)^parity(p >> T & xhi) each); DENSE: tile loaded from d.  LAST: scan
+// instead of writing (single-pass spectra, T == 14).
+template <bool SPARSE, bool LAST, int E>
+__global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
+    pass_a_kernel(int32_t* __restrict__ d, int T, long long ntiles,
+                  const uint64_t* __restrict__ sorted, const unsigned* __restrict__ offsets,
+                  unsigned long long xhi, const unsigned long long* __restrict__ total, int kk,
+                  bmm_candidate* __restrict__ cta_out) {
+    extern __shared__ __align__(16) int32_t s[];
+    const int tid = threadIdx.x;
+    WarpTopK<E> top;
+    uint32_t thr = 0xffffffffu;
+    long long N = 0;
+    if (LAST) {
+        top.init();
+        N = (long long)*total;
+    }
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        int32_t* gt = d + (size_t)tile * kTile;
+        if (SPARSE) {
+            const unsigned b0 = offsets[tile], b1 = offsets[tile + 1];
+            if (b0 == b1 && !LAST) {  // empty tile: its transform is zero
+                int4* g4 = reinterpret_cast<int4*>(gt);
+                for (int i = tid; i < kTile / 4; i += kThr)
+                    g4[i] = make_int4(0, 0, 0, 0);
+                continue;
+            }
+            int4* s4 = reinterpret_cast<int4*>(s);
+            for (int i = tid; i < kTile / 4; i += kThr)
+                s4[i] = make_int4(0, 0, 0, 0);
+            __syncthreads();
+            for (unsigned i = b0 + tid; i < b1; i += kThr) {
+                const uint64_t p = sorted[i];
+                const int v = (T < 64 && (__popcll((p >> T) & xhi) & 1)) ? -1 : 1;
+                atomicAdd(s + swz((int)(p & (kTile - 1))), v);
+            }
+        } else {
+            int32_t v[64];
+#pragma unroll
+            for (int u = 0; u < 64; ++u)
+                v[u] = gt[u * kThr + tid];
+#pragma unroll
+            for (int u = 0; u < 64; ++u)
+                s[swz(u * kThr + tid)] = v[u];
+        }
+        __syncthreads();
+        int32_t x[64];
+        round_load<0, 0, 6>(s, x);
+        round_store<0>(s, x);
+        __syncthreads();
+        round_load<6, 0, 6>(s, x);
+        round_store<6>(s, x);
+        __syncthreads();
+        round_load<8, 4, 2>(s, x);  // element k = (e << 8) | tid
+        if (LAST) {
+            const uint64_t tbase = (uint64_t)tile << kTileLog;
+            scan_values<8, E>(x, N, kk, top, thr,
+                              [&](int k) { return (xhi << T) | tbase | (uint64_t)k; });
+        } else {
+#pragma unroll
+            for (int e = 0; e < 64; ++e)
+                gt[(e << 8) | tid] = x[e];  // coalesced: consecutive tid
+        }
+        __syncthreads();
+    }
+    if (LAST)
+        cta_list_out<E>(top, thr, kk, reinterpret_cast<bmm_candidate*>(s),
+                        cta_out + (size_t)blockIdx.x * kk);
+}
+
+// Middle / last pass over bits [lo, lo + R), R <= 9: tile = 2^R rows
+// (stride 2^lo) x 2^B consecutive elements, B = 14 - R >= 5.
+template <int R, bool LAST, int E>
+__global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
+    pass_mid_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
+                    const unsigned long long* __restrict__ total, int kk,
+                    bmm_candidate* __restrict__ cta_out) {
+    static_assert(R >= 1 && R <= 9, "R in [1, 9]");
+    constexpr int B = kTileLog - R;
+    extern __shared__ __align__(16) int32_t s[];
+    const int tid = threadIdx.x;
+    const long long lowblocks = 1ll << (lo - B);
+    const long long ntiles = (1ll << T) >> kTileLog;
+    WarpTopK<E> top;
+    uint32_t thr = 0xffffffffu;
+    long long N = 0;
+    if (LAST) {
+        top.init();
+        N = (long long)*total;
+    }
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const long long lb = tile % lowblocks, hi = tile / lowblocks;
+        const uint64_t gbase = ((uint64_t)hi << (lo + R)) | ((uint64_t)lb << B);
+        auto gidx = [&](int k) -> uint64_t {
+            return gbase | ((uint64_t)(k >> B) << lo) | (uint64_t)(k & ((1 << B) - 1));
+        };
+        // round 1 works on k = (e << 8) | tid: load it straight from HBM
+        // (a warp reads 32 consecutive elements of one row: full lines)
+        int32_t x[64];
+#pragma unroll
+        for (int e = 0; e < 64; ++e)
+            x[e] = d[gidx((e << 8) | tid)];
+        if constexpr (R > 6) {
+            bfly<0, 6>(x);  // k bits 8..13 = the top six stage bits
+            round_store<8>(s, x);
+            __syncthreads();
+            round_load<2, B - 2, R - 6>(s, x);
+            if (LAST) {
+                scan_values<2, E>(x, N, kk, top, thr,
+                                  [&](int k) { return (xhi << T) | gidx(k); });
+            } else {
+                round_store<2>(s, x);
+                __syncthreads();
+#pragma unroll
+                for (int e = 0; e < 64; ++e) {
+                    const int k = (e << 8) | tid;
+                    d[gidx(k)] = s[swz(k)];
+                }
+            }
+        } else {
+            bfly<B - 8, R>(x);  // stage bits [B, 14) all inside k bits 8..13
+            if (LAST) {
+                scan_values<8, E>(x, N, kk, top, thr,
+                                  [&](int k) { return (xhi << T) | gidx(k); });
+            } else {
+#pragma unroll
+                for (int e = 0; e < 64; ++e)
+                    d[gidx((e << 8) | tid)] = x[e];
+            }
+        }
+        __syncthreads();
+    }
+    if (LAST)
+        cta_list_out<E>(top, thr, kk, reinterpret_cast<bmm_candidate*>(s),
+                        cta_out + (size_t)blockIdx.x * kk);
+}
+
+// Small spectra (T < 14): one CTA, everything in shared memory.
+template <int E>
+__global__ void __launch_bounds__(kThr)
+    small_spectrum_kernel(const uint64_t* __restrict__ pats,
+                          const unsigned long long* __restrict__ count, int t, int kk,
+                          bmm_candidate* __restrict__ out) {
+    extern __shared__ __align__(16) int32_t s[];
+    const int n = 1 << t;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < n; i += kThr)
+        s[i] = 0;
+    __syncthreads();
+    const unsigned long long cnt = *count;
+    for (unsigned long long i = tid; i < cnt; i += kThr)
+        atomicAdd(s + pats[i], 1);
+    __syncthreads();
+    for (int st = 0; st < t; ++st) {
+        for (int q = tid; q < n / 2; q += kThr) {
+            const int j0 = ((q >> st) << (st + 1)) | (q & ((1 << st) - 1));
+            const int j1 = j0 | (1 << st);
+            const int32_t u = s[j0], v = s[j1];
+            s[j0] = u + v;
+            s[j1] = u - v;
+        }
+        __syncthreads();
+    }
+    WarpTopK<E> top;
+    top.init();
+    uint32_t thr = 0xffffffffu;
+    const long long N = (long long)cnt;
+    for (int b0 = tid & ~31; b0 < n; b0 += kThr) {
+        const int m = b0 + (tid & 31);
+        bool ok = m >= 1 && m < n;
+        uint32_t w = 0xffffffffu;
+        if (ok) {
+            const long long w2 = N - (long long)s[m];
+            ok = w2 >= 0 && (w2 & 1) == 0;
+            w = (uint32_t)(w2 >> 1);
+        }
+        top.offer(ok, w, (uint64_t)m, kk, thr);
+    }
+    __syncthreads();
+    cta_list_out<E>(top, thr, kk, reinterpret_cast<bmm_candidate*>(s), out);
+}
+
+template <typename F>
+int dispatch_e(int kk, F&& f) {
+    if (kk <= 32)
+        return f(std::integral_constant<int, 1>{});
+    if (kk <= 128)
+        return f(std::integral_constant<int, 4>{});
+    if (kk <= 1024)
+        return f(std::integral_constant<int, 32>{});
+    return fail(BMM_EINVAL, "spectrum search: k must be <= 1024");
+}
+
+// Dynamic shared memory of a pass kernel: the 64 KB tile, or for the last
+// pass the larger of the tile and the staging of 8 warp lists of 32*E.
+constexpr size_t pass_smem(bool last, int E) {
+    return last && (size_t)(kThr / 32) * 32 * E * sizeof(bmm_candidate) > kTile * sizeof(int32_t)
+               ? (size_t)(kThr / 32) * 32 * E * sizeof(bmm_candidate)
+               : kTile * sizeof(int32_t);
+}
+
+template <int E>
+int launch_mid(int R, bool last, int32_t* d, int T, int lo, unsigned long long xhi,
+               const unsigned long long* total, int kk, bmm_candidate* lists, int grid,
+               cudaStream_t st) {
+    const size_t smem = pass_smem(last, E);
+#define BMM_MID(RR)                                                                               \
+    case RR: {                                                                                    \
+        auto k = last ? pass_mid_kernel<RR, true, E> : pass_mid_kernel<RR, false, E>;             \
+        BMM_CUDA_TRY(                                                                             \
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
+        k<<<grid, kThr, smem, st>>>(d, T, lo, xhi, total, kk, lists);                             \
+        BMM_CUDA_TRY(cudaGetLastError());                                                         \
+        return BMM_OK;                                                                            \
+    }
+    switch (R) {
+        BMM_MID(1)
+        BMM_MID(2)
+        BMM_MID(3)
+        BMM_MID(4)
+        BMM_MID(5)
+        BMM_MID(6)
+        BMM_MID(7)
+        BMM_MID(8)
+        BMM_MID(9)
+    }
+#undef BMM_MID
+    return fail(BMM_EINVAL, "spectrum: bad pass width");
+}
+
+// Split the bits above the first 14 into passes of at most 9, as even as possible.
+void plan_mid(int T, int* widths, int* n) {
+    const int rest = T - kTileLog;
+    const int passes = (rest + 8) / 9;
+    *n = passes;
+    for (int i = 0; i < passes; ++i)
+        widths[i] = rest / passes + (i < rest % passes ? 1 : 0);
+}
+
+int grid_for(Workspace* ws, long long ntiles) {
+    long long g = (long long)ws->sm_count * 2;  // 2 x 64 KB tiles per SM
+    return (int)(ntiles < g ? ntiles : g);
+}
+
+}  // namespace
+
+int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, long long cols,
+                         int kk, bmm_candidate* d_out, cudaStream_t stream) {
+    if (t < 1 || t > 40)
+        return fail(BMM_EINVAL, "spectrum search: t must be in [1, 40]");
+    const int T = t < 33 ? t : 33;
+    const int H = t - T;
+    void *pats = nullptr, *cnt = nullptr;
+    BMM_TRY(ws_buffer(ws, kSlotAux, (size_t)(cols > 0 ? cols : 1) * 8, &pats));
+    BMM_TRY(ws_buffer(ws, kSlotCounter, 16, &cnt));
+    BMM_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, stream));
+    {
+        long long blocks = (cols + 255) / 256;
+        if (blocks > (long long)ws->sm_count * 8)
+            blocks = (long long)ws->sm_count * 8;
+        patterns_kernel<<<(unsigned)(blocks > 0 ? blocks : 1), 256, 0, stream>>>(
+            d_rows, t, W, cols, (uint64_t*)pats, (unsigned long long*)cnt);
+        BMM_CUDA_TRY(cudaGetLastError());
+    }
+    const unsigned long long* total = (const unsigned long long*)cnt;
+    if (T < kTileLog) {
+        return dispatch_e(kk, [&](auto Ec) -> int {
+            constexpr int E = decltype(Ec)::value;
+            const size_t smem0 = ((size_t)1 << T) * 4;
+            const size_t smem1 = (size_t)8 * 32 * E * sizeof(bmm_candidate);
+            const size_t smem = smem0 > smem1 ? smem0 : smem1;
+            auto k = small_spectrum_kernel<E>;
+            BMM_CUDA_TRY(
+                cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k<<<1, kThr, smem, stream>>>((const uint64_t*)pats, total, t, kk, d_out);
+            BMM_CUDA_TRY(cudaGetLastError());
+            return BMM_OK;
+        });
+    }
+    // bucket the patterns by pass-A tile
+    const long long ntiles = 1ll << (T - kTileLog);
+    void *counts = nullptr, *offsets = nullptr, *cursor = nullptr, *sorted = nullptr;
+    BMM_TRY(ws_buffer(ws, kSlotIdx, (size_t)ntiles * 4, &counts));
+    BMM_TRY(ws_buffer(ws, kSlotExtra0, (size_t)(ntiles + 1) * 4, &offsets));
+    BMM_TRY(ws_buffer(ws, kSlotExtra1, (size_t)ntiles * 4, &cursor));
+    BMM_TRY(ws_buffer(ws, kSlotKeys, (size_t)(cols > 0 ? cols : 1) * 8, &sorted));
+    BMM_CUDA_TRY(cudaMemsetAsync(counts, 0, (size_t)ntiles * 4, stream));
+    const int pblocks = ws->sm_count * 4;
+    tile_count_kernel<<<pblocks, 256, 0, stream>>>((const uint64_t*)pats, total, T,
+                                                   (unsigned*)counts);
+    exclusive_scan_kernel<<<1, 1024, 0, stream>>>((const unsigned*)counts, ntiles,
+                                                  (unsigned*)offsets, (unsigned*)cursor);
+    tile_scatter_kernel<<<pblocks, 256, 0, stream>>>((const uint64_t*)pats, total, T,
+                                                     (unsigned*)cursor, (uint64_t*)sorted);
+    BMM_CUDA_TRY(cudaGetLastError());
+
+    void* spec = nullptr;
+    if (T > kTileLog)
+        BMM_TRY(ws_buffer(ws, kSlotSpec, ((size_t)1 << T) * 4, &spec));
+    int widths[4], nmid = 0;
+    plan_mid(T, widths, &nmid);
+    const int grid_a = grid_for(ws, ntiles);
+    const int grid_m = grid_for(ws, ntiles);  // every pass has 2^(T-14) tiles
+    const int grid_last = nmid ? grid_m : grid_a;
+    const long long slices = 1ll << H;
+    bmm_candidate *lists = nullptr, *slice_lists = nullptr;
+    BMM_TRY(ws_buffer(ws, kSlotCand, (size_t)grid_last * kk * sizeof(bmm_candidate),
+                      (void**)&lists));
+    if (slices > 1)
+        BMM_TRY(ws_buffer(ws, kSlotSlices, (size_t)slices * kk * sizeof(bmm_candidate),
+                          (void**)&slice_lists));
+    const size_t smem = kTile * sizeof(int32_t);
+    return dispatch_e(kk, [&](auto Ec) -> int {
+        constexpr int E = decltype(Ec)::value;
+        for (long long x = 0; x < slices; ++x) {
+            bmm_candidate* dst = slices > 1 ? slice_lists + (size_t)x * kk : d_out;
+            if (nmid == 0) {
+                auto k = pass_a_kernel<true, true, E>;
+                const size_t lsmem = pass_smem(true, E);
+                BMM_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                  (int)lsmem));
+                k<<<grid_a, kThr, lsmem, stream>>>((int32_t*)spec, T, ntiles,
+                                                  (const uint64_t*)sorted,
+                                                  (const unsigned*)offsets, (unsigned long long)x,
+                                                  total, kk, lists);
+                BMM_CUDA_TRY(cudaGetLastError());
+            } else {
+                auto k = pass_a_kernel<true, false, E>;
+                BMM_CUDA_TRY(
+                    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+                k<<<grid_a, kThr, smem, stream>>>((int32_t*)spec, T, ntiles,
+                                                  (const uint64_t*)sorted,
+                                                  (const unsigned*)offsets, (unsigned long long)x,
+                                                  total, kk, lists);
+                BMM_CUDA_TRY(cudaGetLastError());
+                int lo = kTileLog;
+                for (int i = 0; i < nmid; ++i) {
+                    BMM_TRY(launch_mid<E>(widths[i], i == nmid - 1, (int32_t*)spec, T, lo,
+                                          (unsigned long long)x, total, kk, lists, grid_m, stream));
+                    lo += widths[i];
+                }
+            }
+            BMM_TRY(merge_topk_lists(lists, grid_last, kk, dst, stream));
+        }
+        if (slices > 1)
+            BMM_TRY(merge_topk_lists(slice_lists, (int)slices, kk, d_out, stream));
+        return BMM_OK;
+    });
+}
+
+// Dense in-place transform of 2^t int32 (t >= 14) with the same passes.
+int spectrum_dense_fwht(Workspace* ws, int32_t* d, int t, cudaStream_t stream) {
+    const long long ntiles = 1ll << (t - kTileLog);
+    const size_t smem = kTile * sizeof(int32_t);
+    auto ka = pass_a_kernel<false, false, 1>;
+    BMM_CUDA_TRY(cudaFuncSetAttribute(ka, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ka<<<grid_for(ws, ntiles), kThr, smem, stream>>>(d, t, ntiles, nullptr, nullptr, 0, nullptr, 0,
+                                                     nullptr);
+    BMM_CUDA_TRY(cudaGetLastError());
+    int widths[4], nmid = 0;
+    plan_mid(t, widths, &nmid);
+    int lo = kTileLog;
+    for (int i = 0; i < nmid; ++i) {
+        BMM_TRY(launch_mid<1>(widths[i], false, d, t, lo, 0, nullptr, 0, nullptr,
+                              grid_for(ws, ntiles), stream));
+        lo += widths[i];
+    }
+    return BMM_OK;
+}
+
+}  // namespace bmm

@@ -94,6 +94,13 @@ typedef struct bmm_features {
 BMM_API uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, size_t stride,
                                   double p, uint64_t seed, size_t scrambles);
 
+/* Autotuner hook for the per-target Gray-code kernel (no reference
+ * counterpart): hs_blocks = carry-save blocks of 8 words per 64-word lane
+ * (0, 2-6, 8; -1 = built-in policy), chunk_bits = Gray-swept low bits per
+ * prefix (-1 = built-in policy).  Process-wide; results never change, only
+ * speed. */
+BMM_API int bmm_gray_tune(int hs_blocks, int chunk_bits);
+
 /* Roofline probe for the Gray-code kernels: runs a register-only kernel with
  * the per-word work of one Gray step (64-bit XOR, 64-bit POPC, add) over the
  * whole device and returns its rate in 64-bit words per second.  No
@@ -118,8 +125,9 @@ BMM_API int bmm_fwht_i32_dev(int32_t* d_data, size_t n, void* stream);
  * t > max_rows for bmm_fwht_search) is BMM_OK with *out_count == 0, as in the
  * reference. */
 
-/* FwhtSearch: t <= min(max_rows, 30).  BMM_EOVERFLOW if the active column
- * count exceeds INT32_MAX (fwht_search.cpp:77-87). */
+/* FwhtSearch: t <= min(max_rows, 33) (the 2^t int32 spectrum is built in
+ * device memory: 32 GB at t = 33).  BMM_EOVERFLOW when cols exceeds INT32_MAX
+ * (the reference's total-weight limit, fwht_search.cpp:77-87). */
 BMM_API int bmm_fwht_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
                     size_t t, size_t max_rows, size_t k, bmm_candidate* out, size_t* out_count);
 
@@ -129,6 +137,16 @@ BMM_API int bmm_fwht_search(const uint64_t* words, size_t stride, size_t cols, c
 BMM_API int bmm_gray_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
                     size_t t, size_t k, size_t chunk_bits, bmm_candidate* out,
                     size_t* out_count);
+
+/* Meet-in-the-middle search (MitmFwhtSearch / CudaMitmFwhtSearch): the same
+ * exact top-k as bmm_fwht_search for 1 <= t <= 40, k <= 1024.  The low
+ * min(t, 33) bits form a spectrum in device memory; bits above 33 are
+ * enumerated.  low_bits is accepted for interface compatibility (0 or in
+ * [1, t - 1]) and does not change the result.  Exact in int32 for any
+ * column count below 2^31 (no int16 limit). */
+BMM_API int bmm_mitm_search(const uint64_t* words, size_t stride, size_t cols, const uint32_t* win,
+                            size_t t, size_t k, size_t low_bits, bmm_candidate* out,
+                            size_t* out_count);
 
 /* ---- per-target searches ----
  * For each of n_targets targets: minimise popcount(row[targets[i]] ^ XOR of
