@@ -3,10 +3,11 @@
     python -m bmmpy_b200.build [--verbose]
 
 Compiles every ``csrc/*.cu`` for sm_100a only (``-gencode
-arch=compute_100a,code=sm_100a``) with nvcc into one shared library with the
-CUDA runtime linked statically, so the library has no Python or torch
-dependency and travels as a single file.  Rebuilds only when a source is
-newer than the library.
+arch=compute_100a,code=sm_100a``), one nvcc process per file in parallel
+(objects in ``bmmpy_b200/_build/``), and links one shared library with the CUDA
+runtime linked statically, so the library has no Python or torch dependency
+and travels as a single file.  Rebuilds only when a source is newer than the
+library.
 """
 
 from __future__ import annotations
@@ -23,8 +24,9 @@ LIB = os.path.join(HERE, "libbmm_b200.so")
 ROOT = os.path.dirname(HERE)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
-         "-Xcompiler", "-fvisibility=hidden", "-shared", "-cudart", "static"]
+COMPILE_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler",
+                 "-fPIC", "-Xcompiler", "-fvisibility=hidden"]
+LINK_FLAGS = ["-shared", "-cudart", "static"]
 
 
 def nvcc() -> str:
@@ -39,8 +41,7 @@ def sources():
 
 
 def deps():
-    return sources() + sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
-        os.path.join(ROOT, "include", "bmm_b200.h")]
+    return sources() + _headers()
 
 
 def up_to_date() -> bool:
@@ -50,21 +51,48 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in deps())
 
 
-def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
-    if not force and up_to_date():
-        return LIB
-    cmd = [nvcc(), *ARCH, *FLAGS, "-I", os.path.join(ROOT, "include"), "-o", LIB + ".tmp",
-           *sources()]
+def _headers():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cuh"))) + [
+        os.path.join(ROOT, "include", "bmm_b200.h")]
+
+
+def _compile(src: str, ptxas_info: bool, force: bool) -> tuple[str, int, str]:
+    obj = os.path.join(HERE, "_build", os.path.basename(src) + ".o")
+    if not force and not ptxas_info and os.path.exists(obj):
+        t = os.path.getmtime(obj)
+        if all(os.path.getmtime(p) <= t for p in [src, *_headers()]):
+            return obj, 0, ""
+    cmd = [nvcc(), *ARCH, *COMPILE_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src,
+           "-o", obj]
     if ptxas_info:
         cmd[1:1] = ["-Xptxas", "-v"]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    return obj, proc.returncode, proc.stdout + proc.stderr
+
+
+def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) -> str:
+    """Compile each csrc/*.cu in parallel (one nvcc per file), then link."""
+    if not force and up_to_date():
+        return LIB
+    from concurrent.futures import ThreadPoolExecutor
+
+    os.makedirs(os.path.join(HERE, "_build"), exist_ok=True)
+    srcs = sources()
+    with ThreadPoolExecutor(max_workers=max(1, min(len(srcs), os.cpu_count() or 1))) as pool:
+        results = list(pool.map(lambda s: _compile(s, ptxas_info, force), srcs))
+    failed = [out for _, rc, out in results if rc != 0]
+    if verbose or ptxas_info or failed:
+        for _, _, out in results:
+            sys.stderr.write(out)
+    if failed:
+        raise RuntimeError("nvcc failed building libbmm_b200.so")
+    cmd = [nvcc(), *ARCH, *LINK_FLAGS, "-o", LIB + ".tmp", *[o for o, _, _ in results]]
     if verbose:
         print(" ".join(cmd), flush=True)
     proc = subprocess.run(cmd, capture_output=True, text=True)
     if proc.returncode != 0:
         sys.stderr.write(proc.stdout + proc.stderr)
-        raise RuntimeError("nvcc failed building libbmm_b200.so")
-    if verbose or ptxas_info:
-        sys.stderr.write(proc.stderr)
+        raise RuntimeError("nvcc failed linking libbmm_b200.so")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 
