@@ -40,6 +40,16 @@ _szp = C.POINTER(C.c_size_t)
 _vp = C.c_void_p
 _candp = C.POINTER(Candidate_t)
 
+
+class Instance_t(C.Structure):
+    _fields_ = [("word_offset", C.c_uint64), ("rows", C.c_uint32), ("cols", C.c_uint32),
+                ("stride", C.c_uint32), ("k", C.c_uint32), ("out_offset", C.c_uint64)]
+
+
+INSTANCE_DTYPE = np.dtype([("word_offset", np.uint64), ("rows", np.uint32), ("cols", np.uint32),
+                           ("stride", np.uint32), ("k", np.uint32), ("out_offset", np.uint64)])
+_instp = C.POINTER(Instance_t)
+
 # name -> argtypes (all return int unless listed in _RESTYPES)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
@@ -57,6 +67,12 @@ SIGNATURES = {
     "bmm_gray_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, C.c_int, _u64p, _u32p],
     "bmm_gray_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, C.c_int, _vp, _vp, _vp],
     "bmm_gray_targets_noalloc": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, C.c_int, _vp, _vp, _vp],
+    "bmm_batch_create": [_vp, _sz, C.POINTER(_vp)],
+    "bmm_batch_info": [_vp, C.POINTER(C.c_longlong), _szp, C.POINTER(C.c_int)],
+    "bmm_batch_run": [_vp, _vp, _vp, _vp, _vp],
+    "bmm_batch_destroy": [_vp],
+    "bmm_batch_targets": [_u64p, _sz, _vp, _sz, _u64p, _u32p],
+    "bmm_batch_policy": [C.c_int, C.c_int],
     "bmm_fwht_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, _u64p, _u32p],
     "bmm_fwht_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp, _vp],
 }

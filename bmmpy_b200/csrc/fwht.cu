@@ -20,6 +20,7 @@
 //    two butterflies and the top bit is unpacked only at the final stage.
 #include "common.cuh"
 #include "fwht.cuh"
+#include "target_item.cuh"
 
 #include <type_traits>
 #include "topk.cuh"
@@ -74,42 +75,12 @@ __global__ void __launch_bounds__(256)
 // columns count (inactive ones land in bucket 0 with sign +1), so
 // weight(S) = (cols - WHT[S]) / 2.  Result: argmax WHT (smallest S on ties).
 
-// Pattern of column c over the k others, and the target bit.
-__device__ __forceinline__ uint32_t col_pattern(const uint64_t* __restrict__ words, int stride,
-                                                const uint32_t* oth, int k, uint32_t tgt, int c,
-                                                int* tbit) {
-    const int w = c >> 6, bit = c & 63;
-    uint32_t p = 0;
-    for (int j = 0; j < k; ++j)
-        p |= (uint32_t)((__ldg(words + (size_t)oth[j] * stride + w) >> bit) & 1ull) << j;
-    *tbit = (int)((__ldg(words + (size_t)tgt * stride + w) >> bit) & 1ull);
-    return p;
-}
+struct ListOthers {
+    const uint32_t* oth;
+    __device__ __forceinline__ uint32_t operator()(int j) const { return oth[j]; }
+};
 
-// Packed-pair transform for k = 16: 2^15 int32 in smem, 512 threads, 64
-// elements per thread held in registers for three rounds (bits 0-5, 6-11,
-// 12-14).  Exact for cols <= 32767.
-constexpr int kT16 = 512;
-
-// Bank swizzle of the packed spectrum: element i lives at i ^ ((i >> 6) & 31),
-// which makes all three register rounds below conflict-free.
-__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 6) & 31); }
-
-__device__ __forceinline__ void bfly64(int32_t (&x)[64], int lo_bit, int nbits) {
-#pragma unroll
-    for (int s = 0; s < 6; ++s) {
-        if (s < nbits) {
-            const int h = 1 << (s + lo_bit);
-#pragma unroll
-            for (int e = 0; e < 64; ++e)
-                if ((e & h) == 0) {
-                    const int32_t u = x[e], v = x[e | h];
-                    x[e] = u + v;
-                    x[e | h] = u - v;
-                }
-        }
-    }
-}
+constexpr int kT16 = item::kFwht16Threads;
 
 __global__ void __launch_bounds__(kT16, 1)
     fwht_targets16_kernel(const uint64_t* __restrict__ words, int stride, int cols,
@@ -118,94 +89,12 @@ __global__ void __launch_bounds__(kT16, 1)
                           uint32_t* __restrict__ best_weight) {
     extern __shared__ __align__(16) int32_t P[];  // 32768 packed entries
     __shared__ uint32_t red[kT16 / 32];
-    constexpr int k = 16;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const uint32_t* oth = others + (size_t)item * k;
-        const uint32_t tgt = targets[item];
-        int4* P4 = reinterpret_cast<int4*>(P);
-        for (int i = tid; i < 32768 / 4; i += kT16)
-            P4[i] = make_int4(0, 0, 0, 0);
-        __syncthreads();
-        // signed packed histogram
-        for (int c = tid; c < cols; c += kT16) {
-            int tb;
-            const uint32_t p = col_pattern(words, stride, oth, k, tgt, c, &tb);
-            const int32_t one = (p & 0x8000u) ? 65536 : 1;
-            atomicAdd(P + swz((int)(p & 0x7fffu)), tb ? -one : one);
-        }
-        __syncthreads();
-        int32_t x[64];
-        // round 1: bits 0-5, element = tid*64 + e
-        {
-#pragma unroll
-            for (int e = 0; e < 64; ++e)
-                x[e] = P[swz((tid << 6) | e)];
-            bfly64(x, 0, 6);
-#pragma unroll
-            for (int e = 0; e < 64; ++e)
-                P[swz((tid << 6) | e)] = x[e];
-        }
-        __syncthreads();
-        // round 2: bits 6-11, element = (tid>>6)<<12 | e<<6 | (tid&63)
-        {
-            const int basei = ((tid >> 6) << 12) | (tid & 63);
-#pragma unroll
-            for (int e = 0; e < 64; ++e)
-                x[e] = P[swz(basei | (e << 6))];
-            bfly64(x, 0, 6);
-#pragma unroll
-            for (int e = 0; e < 64; ++e)
-                P[swz(basei | (e << 6))] = x[e];
-        }
-        __syncthreads();
-        // round 3: bits 12-14; element = eh<<12 | tid<<3 | el, x[eh*8 + el]
-        {
-#pragma unroll
-            for (int e = 0; e < 64; ++e)
-                x[e] = P[swz(((e >> 3) << 12) | (tid << 3) | (e & 7))];
-            bfly64(x, 3, 3);
-        }
-        // unpack the top bit, find max WHT with the smallest S
-        int32_t best_v = INT32_MIN;
-        uint32_t best_s = 0xffffffffu;
-#pragma unroll
-        for (int e = 0; e < 64; ++e) {
-            const int32_t pk = x[e];
-            const int32_t lo = (int32_t)(int16_t)(pk & 0xffff);
-            const int32_t hi = (pk - lo) >> 16;
-            const uint32_t s0 = (uint32_t)(((e >> 3) << 12) | (tid << 3) | (e & 7));
-            const int32_t v0 = lo + hi, v1 = lo - hi;
-            if (v0 > best_v || (v0 == best_v && s0 < best_s))
-                best_v = v0, best_s = s0;
-            if (v1 > best_v || (v1 == best_v && (s0 | 0x8000u) < best_s))
-                best_v = v1, best_s = s0 | 0x8000u;
-        }
-        // key: larger v first, then smaller s
-        uint32_t key = ((uint32_t)(best_v + 32768) << 16) | (0xffffu - best_s);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
-            key = max(key, __shfl_xor_sync(kFull, key, o));
-        if (lane == 0)
-            red[warp] = key;
-        __syncthreads();
-        if (warp == 0) {
-            uint32_t kv = lane < kT16 / 32 ? red[lane] : 0u;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-                kv = max(kv, __shfl_xor_sync(kFull, kv, o));
-            if (lane == 0) {
-                const int32_t v = (int32_t)(kv >> 16) - 32768;
-                best_mask[item] = 0xffffu - (kv & 0xffffu);
-                best_weight[item] = (uint32_t)((cols - v) / 2);
-            }
-        }
-        __syncthreads();
-    }
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x)
+        item::fwht16(P, red, words, stride, cols, ListOthers{others + (size_t)it * 16}, targets[it],
+                     best_mask + it, best_weight + it);
 }
 
-// Generic per-target transform for k <= 15 (and any k when cols forbids
-// packing is excluded by the host): int32 spectrum of 2^k in smem.
+// k <= 15: int32 spectrum of 2^k in smem.
 __global__ void __launch_bounds__(256)
     fwht_targets_small_kernel(const uint64_t* __restrict__ words, int stride, int cols,
                               const uint32_t* __restrict__ targets,
@@ -214,53 +103,9 @@ __global__ void __launch_bounds__(256)
                               uint32_t* __restrict__ best_weight) {
     extern __shared__ __align__(16) int32_t S[];
     __shared__ unsigned long long red[8];
-    const int n = 1 << k;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    for (int item = blockIdx.x; item < n_items; item += gridDim.x) {
-        const uint32_t* oth = others + (size_t)item * k;
-        const uint32_t tgt = targets[item];
-        for (int i = tid; i < n; i += blockDim.x)
-            S[i] = 0;
-        __syncthreads();
-        for (int c = tid; c < cols; c += blockDim.x) {
-            int tb;
-            const uint32_t p = col_pattern(words, stride, oth, k, tgt, c, &tb);
-            atomicAdd(S + p, tb ? -1 : 1);
-        }
-        __syncthreads();
-        for (int st = 0; st < k; ++st) {
-            for (int q = tid; q < n / 2; q += blockDim.x) {
-                const int j0 = ((q >> st) << (st + 1)) | (q & ((1 << st) - 1));
-                const int j1 = j0 | (1 << st);
-                const int32_t u = S[j0], v = S[j1];
-                S[j0] = u + v;
-                S[j1] = u - v;
-            }
-            __syncthreads();
-        }
-        // key: (v + 2^31) << 32 | ~s  -> max
-        unsigned long long key = 0;
-        for (int s = tid; s < n; s += blockDim.x) {
-            const unsigned long long kk =
-                ((unsigned long long)(uint32_t)(S[s] + 0x80000000u) << 32) | (0xffffffffu - (uint32_t)s);
-            key = kk > key ? kk : key;
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const unsigned long long ot = __shfl_xor_sync(kFull, key, o);
-            key = ot > key ? ot : key;
-        }
-        if (lane == 0)
-            red[warp] = key;
-        __syncthreads();
-        if (tid == 0) {
-            unsigned long long kv = 0;
-            for (int i = 0; i < (int)(blockDim.x >> 5); ++i)
-                kv = red[i] > kv ? red[i] : kv;
-            const int32_t v = (int32_t)((uint32_t)(kv >> 32) - 0x80000000u);
-            best_mask[item] = 0xffffffffu - (uint32_t)(kv & 0xffffffffu);
-            best_weight[item] = (uint32_t)(((long long)cols - v) / 2);
-        }
+    for (int it = blockIdx.x; it < n_items; it += gridDim.x) {
+        item::fwht_small(S, red, words, stride, cols, ListOthers{others + (size_t)it * k}, k,
+                         targets[it], best_mask + it, best_weight + it);
         __syncthreads();
     }
 }

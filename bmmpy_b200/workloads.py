@@ -8,8 +8,8 @@ library's xorshift64 generator (``bmm_gen_instance``).
 * ``c3``: 512x65536 Bernoulli(0.02), seed 2, 2000 row-XOR scrambles; windows
   of 32 consecutive rows.
 * ``c4``: batch instance idx in [0, 4096): n x m with n, m log-uniform in
-  [16, 128] x [64, 2048] (xorshift64 seeded 1000+idx+0x10000, two unit
-  draws), Bernoulli(0.05) seeded 1000+idx, 4n scrambles; k = min(n-1, 16).
+  [16, 128] x [64, 2048] (xorshift64 seeded 1000+idx+0x10000, 8 draws
+  discarded, then two unit draws), Bernoulli(0.05) seeded 1000+idx, 4n scrambles; k = min(n-1, 16).
 """
 
 from __future__ import annotations
@@ -43,7 +43,10 @@ def _xs(x: int) -> int:
 
 
 def batch_shape(idx: int) -> tuple[int, int]:
-    st = _xs(C4["seed0"] + idx + 0x10000)
+    st = C4["seed0"] + idx + 0x10000
+    for _ in range(8):  # small seeds leave the first draws tiny: discard them
+        st = _xs(st)
+    st = _xs(st)
     u1 = (st >> 11) / 9007199254740992.0
     st = _xs(st)
     u2 = (st >> 11) / 9007199254740992.0

@@ -101,6 +101,46 @@ BMM_API uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, siz
  * speed. */
 BMM_API int bmm_gray_tune(int hs_blocks, int chunk_bits);
 
+/* ---- batched per-target searches (thousands of uneven instances) ----
+ * Instance i is a rows x cols matrix stored at words + word_offset with
+ * `stride` words per row; every row r is a target searched against the k
+ * others (r + 1 + j) mod rows, j < k (1 <= k <= min(16, rows - 1)); its
+ * result goes to best_mask/best_weight[out_offset + r] (S over the others,
+ * ties to the smallest S, as bmm_gray_targets).  One persistent launch with
+ * a global work queue; the plan orders items longest first and picks per
+ * shape the transform (cols <= 32767) or the Gray enumeration (cols <= 512)
+ * by the policy below. */
+typedef struct bmm_instance {
+    uint64_t word_offset;
+    uint32_t rows;
+    uint32_t cols;
+    uint32_t stride;
+    uint32_t k;
+    uint64_t out_offset;
+} bmm_instance;
+
+typedef struct bmm_batch bmm_batch;
+
+/* Plan a batch from host descriptors (allocates the plan's device copy). */
+BMM_API int bmm_batch_create(const bmm_instance* inst, size_t n_inst, bmm_batch** out);
+/* items, output length, items per method {transform k=16, transform k<16,
+ * Gray} of a plan. */
+BMM_API int bmm_batch_info(const bmm_batch* b, long long* n_items, size_t* n_out, int* methods3);
+/* Run on device buffers (asynchronous on `stream`).  The work-queue reset and
+ * the kernel are a CUDA graph captured on the first run and replayed; new
+ * buffer pointers trigger one re-capture. */
+BMM_API int bmm_batch_run(bmm_batch* b, const uint64_t* d_words, uint64_t* d_best_mask,
+                          uint32_t* d_best_weight, void* stream);
+BMM_API int bmm_batch_destroy(bmm_batch* b);
+/* Host-buffer convenience: plan, upload, run, download (synchronous). */
+BMM_API int bmm_batch_targets(const uint64_t* words, size_t n_words, const bmm_instance* inst,
+                              size_t n_inst, uint64_t* best_mask, uint32_t* best_weight);
+/* Autotuner hook (no reference counterpart): k = 16 items whose rows have at
+ * most gray_max_words words (0..8) use the Gray enumeration instead of the
+ * transform; force_method (-1 none, 0/1 transform, 2 Gray) overrides where
+ * legal.  Applies to plans created afterwards; results never change. */
+BMM_API int bmm_batch_policy(int gray_max_words, int force_method);
+
 /* Roofline probe for the Gray-code kernels: runs a register-only kernel with
  * the per-word work of one Gray step (64-bit XOR, 64-bit POPC, add) over the
  * whole device and returns its rate in 64-bit words per second.  No

@@ -74,8 +74,11 @@ def _xs(state):
 
 def batch_shape(idx: int):
     """(n, m) of batch instance idx: n, m log-uniform in [16,128] x [64,2048],
-    drawn with xorshift64 seeded 1000+idx+0x10000 (two unit doubles)."""
+    drawn with xorshift64 seeded 1000+idx+0x10000 (8 draws discarded, then
+    two unit doubles)."""
     st = C4["seed0"] + idx + 0x10000
+    for _ in range(8):  # small seeds leave the first draws tiny: discard them
+        st = _xs(st)
     st = _xs(st)
     u1 = (st >> 11) / 9007199254740992.0
     st = _xs(st)

@@ -100,18 +100,40 @@ def per_target(R, m, cols, rows, k, offset=1):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-slow", action="store_true")
+    ap.add_argument("--only", default="", help="comma list of c1,c2,c3,c4,ka to regenerate; "
+                    "the other entries of workloads.npz are kept")
     args = ap.parse_args()
+    only = set(filter(None, args.only.split(",")))
+    want = (lambda name: not only or name in only)
     R = ref()
     if R is None:
         raise SystemExit("build the reference first: make -C oracle ref")
     P = port()
 
-    ka = known_answers(R)
-    with open(os.path.join(HERE, "known_answers.json"), "w") as f:
-        json.dump(ka, f, indent=1)
-    print("known_answers.json written")
+    if want("ka"):
+        ka = known_answers(R)
+        with open(os.path.join(HERE, "known_answers.json"), "w") as f:
+            json.dump(ka, f, indent=1)
+        print("known_answers.json written")
 
     arrays = {}
+    npz = os.path.join(HERE, "workloads.npz")
+    if only and os.path.exists(npz):
+        arrays.update(dict(np.load(npz)))
+    t0 = time.time()
+    if want("c1"):
+        c1(R, P, arrays)
+    if want("c2"):
+        c2(R, P, arrays)
+    if want("c4"):
+        c4(R, P, arrays)
+    if want("c3") and not args.skip_slow:
+        c3(R, P, arrays)
+    np.savez_compressed(npz, **arrays)
+    print("workloads.npz written")
+
+
+def c1(R, P, arrays):
     t0 = time.time()
     m, _ = P.gen_instance(C1["rows"], C1["cols"], C1["p"], C1["seed"])
     arrays["c1_mask"], arrays["c1_weight"] = per_target(R, m, C1["cols"], C1["rows"], C1["k"])
@@ -123,6 +145,8 @@ def main():
     arrays["c1_row0_window_best"] = np.array(best0, np.uint64)
     print("C1 done", time.time() - t0)
 
+
+def c2(R, P, arrays):
     t0 = time.time()
     m, _ = P.gen_instance(C2["rows"], C2["cols"], C2["p"], C2["seed"])
     arrays["c2_mask"], arrays["c2_weight"] = per_target(R, m, C2["cols"], C2["rows"], C2["k"])
@@ -130,6 +154,8 @@ def main():
     arrays["c2k16_mask"], arrays["c2k16_weight"] = per_target(R, m, C2["cols"], C2["rows"], 16)
     print("C2 done", time.time() - t0)
 
+
+def c4(R, P, arrays):
     t0 = time.time()
     sums = []
     first = []
@@ -144,20 +170,18 @@ def main():
     arrays["c4_first32"] = np.concatenate(first, 0)
     print("C4 done", time.time() - t0)
 
-    if not args.skip_slow:
-        t0 = time.time()
-        m, planted = P.gen_instance(C3["rows"], C3["cols"], C3["p"], C3["seed"], C3["scrambles"])
-        arrays["c3_planted"] = np.array([planted], np.uint64)
-        tops = []
-        for j in range(C3["golden_windows"]):
-            res = R.mitm_search(m, C3["cols"], list(range(32 * j, 32 * j + 32)), 64)
-            tops.append(np.array(res, np.uint64))
-            print("  C3 window", j, time.time() - t0)
-        arrays["c3_top64"] = np.stack(tops, 0)
-        print("C3 done", time.time() - t0)
 
-    np.savez_compressed(os.path.join(HERE, "workloads.npz"), **arrays)
-    print("workloads.npz written")
+def c3(R, P, arrays):
+    t0 = time.time()
+    m, planted = P.gen_instance(C3["rows"], C3["cols"], C3["p"], C3["seed"], C3["scrambles"])
+    arrays["c3_planted"] = np.array([planted], np.uint64)
+    tops = []
+    for j in range(C3["golden_windows"]):
+        res = R.mitm_search(m, C3["cols"], list(range(32 * j, 32 * j + 32)), 64)
+        tops.append(np.array(res, np.uint64))
+        print("  C3 window", j, time.time() - t0)
+    arrays["c3_top64"] = np.stack(tops, 0)
+    print("C3 done", time.time() - t0)
 
 
 if __name__ == "__main__":
