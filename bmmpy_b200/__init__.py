@@ -2,14 +2,27 @@
 
 Same public names as bmmpy for the search / FWHT path: build a BitMatrix,
 take a RowWindow, run a searcher, get Candidates ordered by (weight, mask).
-Every search runs on the GPU through libbmm_b200.so; there is no CPU
+The genetic optimizers (GeneticAlgorithm, IslandModel) run whole generations
+on the device.  Every search runs on the GPU through libbmm_b200.so; there is no CPU
 fallback (importing the package works without a GPU, calling a search
 does not).
 """
 
 from __future__ import annotations
 
+from . import ga
 from .candidate import Candidate
+from .ga import (
+    GeneticAlgorithm,
+    IslandModel,
+    IslandModelSnapshot,
+    IslandSnapshot,
+    IslandSpec,
+    MigrationPolicy,
+    OverflowPolicy,
+    RunStats,
+    StopCriteria,
+)
 from .matrix import BitMatrix, RowWindow, matrix_from_rows
 from .runtime import RuntimeFeatures, fwht_i16, fwht_i32, get_runtime_features, get_version
 from .search import (
@@ -27,7 +40,16 @@ __all__ = [
     "CudaBruteforceSearch",
     "CudaMitmFwhtSearch",
     "FwhtSearch",
+    "GeneticAlgorithm",
+    "IslandModel",
+    "IslandModelSnapshot",
+    "IslandSnapshot",
+    "IslandSpec",
+    "MigrationPolicy",
     "MitmFwhtSearch",
+    "OverflowPolicy",
+    "RunStats",
+    "StopCriteria",
     "RowWindow",
     "RuntimeFeatures",
     "fwht_i16",

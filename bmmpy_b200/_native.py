@@ -50,6 +50,35 @@ INSTANCE_DTYPE = np.dtype([("word_offset", np.uint64), ("rows", np.uint32), ("co
                            ("stride", np.uint32), ("k", np.uint32), ("out_offset", np.uint64)])
 _instp = C.POINTER(Instance_t)
 
+GA_STOP_MAX_GENERATIONS, GA_STOP_MAX_STALE, GA_STOP_TARGET = 1, 2, 4
+
+
+class GaConfig_t(C.Structure):
+    """bmm_ga_config (GeneticAlgorithmConfig)."""
+
+    _fields_ = [("population_size", C.c_uint32), ("elite_count", C.c_uint32),
+                ("num_parents", C.c_uint32), ("num_offspring", C.c_uint32),
+                ("tournament_size", C.c_uint32), ("enable_catastrophe", C.c_uint32),
+                ("catastrophe_threshold", C.c_uint32), ("flags", C.c_uint32),
+                ("catastrophe_survival_rate", C.c_double), ("mutation_rate", C.c_double),
+                ("max_generations", C.c_uint64), ("max_stale_generations", C.c_uint64),
+                ("target_total_weight", C.c_uint64), ("seed", C.c_uint64)]
+
+
+class GaMigration_t(C.Structure):
+    """bmm_ga_migration (MigrationPolicy subset)."""
+
+    _fields_ = [("interval_generations", C.c_uint32), ("import_count", C.c_uint32)]
+
+
+class GaStats_t(C.Structure):
+    """bmm_ga_island_stats (RunStats plus the island's best score)."""
+
+    _fields_ = [("generations", C.c_uint64), ("evaluations", C.c_uint64),
+                ("stale_generations", C.c_uint64), ("seed", C.c_uint64),
+                ("best_score", C.c_uint64), ("done", C.c_uint32),
+                ("no_improvement", C.c_uint32), ("mutation_rate", C.c_double)]
+
 # name -> argtypes (all return int unless listed in _RESTYPES)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
@@ -75,6 +104,17 @@ SIGNATURES = {
     "bmm_batch_policy": [C.c_int, C.c_int],
     "bmm_fwht_targets": [_u64p, _sz, _sz, _sz, _u32p, _u32p, _sz, _sz, _u64p, _u32p],
     "bmm_fwht_targets_dev": [_vp, _sz, _sz, _sz, _vp, _vp, _sz, _sz, _vp, _vp, _vp],
+    "bmm_ga_create": [_u64p, _sz, _sz, _szp, _sz, C.POINTER(GaConfig_t), _sz,
+                      C.POINTER(GaMigration_t), C.POINTER(_vp)],
+    "bmm_ga_run": [_vp, C.c_uint64, C.c_uint32, _u64p, C.POINTER(C.c_int)],
+    "bmm_ga_stats": [_vp, _sz, C.POINTER(GaStats_t)],
+    "bmm_ga_best": [_vp, _sz, _u64p, _u32p, _u64p],
+    "bmm_ga_population": [_vp, _sz, _u64p, _u32p, _u64p],
+    "bmm_ga_destroy": [_vp],
+    "bmm_ga_eval": [_u64p, _sz, _sz, _szp, _sz, _u64p, _sz, _u32p],
+    "bmm_ga_mutate": [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, C.c_double, _u64p],
+    "bmm_ga_local_improve": [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p],
+    "bmm_ga_crossover": [_sz, _sz, _u64p, _u32p, _u64p, _u32p],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
              "bmm_gen_instance": C.c_uint64}
@@ -131,6 +171,10 @@ def u64p(a):
 
 def u32p(a):
     return ptr(a, _u32p)
+
+
+def szp(a):
+    return ptr(a, _szp)
 
 
 def candp(a):

@@ -19,9 +19,12 @@
  *                        row i and k other rows, the reference window search
  *                        over [i, o_1..o_k] restricted to masks with bit 0 set
  *                        (best = (S << 1) | 1 in the reference's mask order).
- *   bmm_ga_*             GeneticAlgorithm fitness evaluation and mutation
+ *   bmm_ga_*             GeneticAlgorithm / IslandModel (whole generations on the
+ *                        device) and their operators
+ *                        src/ga/genetic_algorithm_lifecycle.cpp:16-200,
+ *                        src/ga/genetic_algorithm_operators.cpp:15-192,
  *                        src/ga/genetic_algorithm_internal.hpp:41-103,
- *                        src/ga/genetic_algorithm_operators.cpp:100-192.
+ *                        src/ga/island.cpp:149-228.
  *
  * Conventions
  *  - Every function returns an int status (BMM_OK == 0, negative on error)
@@ -226,6 +229,89 @@ BMM_API int bmm_fwht_targets(const uint64_t* words, size_t rows, size_t stride, 
 BMM_API int bmm_fwht_targets_dev(const uint64_t* d_words, size_t rows, size_t stride, size_t cols,
                          const uint32_t* d_targets, const uint32_t* d_others, size_t n_targets,
                          size_t k, uint64_t* d_best_mask, uint32_t* d_best_weight, void* stream);
+
+/* ---- Genetic algorithm (island model) ------------------------------------
+ * Replaces bmmpy::ga::GeneticAlgorithm (include/bmmpy/ga/genetic_algorithm.hpp:17-88)
+ * and bmmpy::ga::IslandModel (include/bmmpy/ga/island_model.hpp:16-53) for
+ * windows of at most 256 rows, populations of at most 1024.  An individual
+ * is n candidate masks of ceil(n/64) words each (Candidate::mask) plus a
+ * weight per candidate; its fitness is the sum of the weights.  Every island
+ * draws from its own xorshift64 stream exactly as GeneticAlgorithm does, so
+ * a single island reproduces GeneticAlgorithm::step() trajectories for the
+ * same seed.  Islands exchange their best individual along a ring: island i
+ * imports island i-1's best whenever island i-1's migration interval divides
+ * its generation count; import_migrants rules apply (lifecycle.cpp:83-110). */
+#define BMM_GA_STOP_MAX_GENERATIONS 1u /* StopCriteria::max_generations is set */
+#define BMM_GA_STOP_MAX_STALE 2u       /* StopCriteria::max_stale_generations is set */
+#define BMM_GA_STOP_TARGET 4u          /* StopCriteria::target_total_weight is set */
+typedef struct bmm_ga_config { /* GeneticAlgorithmConfig (genetic_algorithm.hpp:17-29) */
+    uint32_t population_size;  /* these eight must agree across islands */
+    uint32_t elite_count;
+    uint32_t num_parents;      /* 1..4 */
+    uint32_t num_offspring;    /* >= 1 */
+    uint32_t tournament_size;
+    uint32_t enable_catastrophe;
+    uint32_t catastrophe_threshold;
+    uint32_t flags;            /* BMM_GA_STOP_* (per island) */
+    double catastrophe_survival_rate;
+    double mutation_rate;      /* per island */
+    uint64_t max_generations;  /* per island */
+    uint64_t max_stale_generations;
+    uint64_t target_total_weight;
+    uint64_t seed;             /* per island */
+} bmm_ga_config;
+typedef struct bmm_ga_migration { /* MigrationPolicy (ga/types.hpp:28-33) subset */
+    uint32_t interval_generations; /* 0: never export */
+    uint32_t import_count;         /* 0: never import */
+} bmm_ga_migration;
+typedef struct bmm_ga_island_stats { /* RunStats (ga/types.hpp:20-25) + IslandSnapshot */
+    uint64_t generations;
+    uint64_t evaluations;
+    uint64_t stale_generations;
+    uint64_t seed;
+    uint64_t best_score;
+    uint32_t done;
+    uint32_t no_improvement;
+    double mutation_rate;
+} bmm_ga_island_stats;
+typedef struct bmm_ga bmm_ga;
+/* initialize(window) of `islands` islands, cfgs[i] configuring island i;
+ * migration: one policy per island, or NULL (islands never exchange).
+ * win: n row indices into words. */
+BMM_API int bmm_ga_create(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                          size_t n, const bmm_ga_config* cfgs, size_t islands,
+                          const bmm_ga_migration* migration, bmm_ga** out);
+/* Up to `generations` step()s of every island not done; the host checks the
+ * stop flags every check_every generations (0 = 1).  *ran: generations run. */
+BMM_API int bmm_ga_run(bmm_ga* g, uint64_t generations, uint32_t check_every, uint64_t* ran,
+                       int* all_done);
+BMM_API int bmm_ga_stats(bmm_ga* g, size_t island, bmm_ga_island_stats* out);
+/* best_individual(): island (SIZE_MAX: the model's best, first strict
+ * minimum over islands); masks n*ceil(n/64) words, weights n. */
+BMM_API int bmm_ga_best(bmm_ga* g, size_t island, uint64_t* masks, uint32_t* weights,
+                        uint64_t* score);
+/* The island's current population in order: masks P*n*ceil(n/64) words,
+ * weights P*n, fitness P (each may be NULL). */
+BMM_API int bmm_ga_population(bmm_ga* g, size_t island, uint64_t* masks, uint32_t* weights,
+                              uint64_t* fitness);
+BMM_API int bmm_ga_destroy(bmm_ga* g);
+/* Operators on one individual, through the same device code as the
+ * generation kernels.  eval: internal::eval_cand_weight
+ * (genetic_algorithm_internal.hpp:41-103) of `count` masks.  mutate:
+ * GeneticAlgorithm::mutate (operators.cpp:100-129) with the generator state
+ * in/out (0 = the default seed).  local_improve: local_improvement
+ * (operators.cpp:131-192).  crossover: crossover (operators.cpp:58-98) of
+ * `parents` individuals laid out one after another. */
+BMM_API int bmm_ga_eval(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                        size_t n, const uint64_t* masks, size_t count, uint32_t* weights);
+BMM_API int bmm_ga_mutate(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                          size_t n, uint64_t* masks, uint32_t* weights, double mutation_rate,
+                          uint64_t* rng_state);
+BMM_API int bmm_ga_local_improve(const uint64_t* words, size_t stride, size_t cols,
+                                 const size_t* win, size_t n, uint64_t* masks, uint32_t* weights);
+BMM_API int bmm_ga_crossover(size_t n, size_t parents, const uint64_t* parent_masks,
+                             const uint32_t* parent_weights, uint64_t* child_masks,
+                             uint32_t* child_weights);
 
 #ifdef __cplusplus
 }

@@ -582,3 +582,374 @@ void orc_local_improvement(const uint64_t* words, size_t stride, size_t cols, co
     }
     free(mat);
 }
+
+/* ---- GA crossover (src/ga/genetic_algorithm_operators.cpp:58-98) and the
+ * PivotBasis it fills (include/bmmpy/core/detail/xor_basis.hpp:117-155). ---- */
+static int highest_bit_words(const uint64_t* v, size_t mw) {
+    for (size_t w = mw; w-- > 0;)
+        if (v[w])
+            return (int)(w * 64 + 63 - __builtin_clzll(v[w]));
+    return -1;
+}
+
+/* Greedy insertion with the pivot at the highest set bit; returns 1 when
+ * the vector was independent (stored at its pivot), 0 otherwise. */
+static int pivot_try_insert(uint64_t* basis, unsigned char* used, const uint64_t* cand, size_t mw,
+                            uint64_t* tmp) {
+    memcpy(tmp, cand, mw * sizeof(uint64_t));
+    for (;;) {
+        const int hb = highest_bit_words(tmp, mw);
+        if (hb < 0)
+            return 0;
+        if (!used[hb]) {
+            used[hb] = 1;
+            memcpy(basis + (size_t)hb * mw, tmp, mw * sizeof(uint64_t));
+            return 1;
+        }
+        for (size_t w = 0; w < mw; ++w)
+            tmp[w] ^= basis[(size_t)hb * mw + w];
+    }
+}
+
+typedef struct {
+    uint32_t weight;
+    uint32_t pc;
+    size_t idx;
+} orc_pool_entry;
+
+static int pool_cmp(const void* a, const void* b) {
+    const orc_pool_entry* x = (const orc_pool_entry*)a;
+    const orc_pool_entry* y = (const orc_pool_entry*)b;
+    if (x->weight != y->weight)
+        return x->weight < y->weight ? -1 : 1;
+    if (x->pc != y->pc)
+        return x->pc < y->pc ? -1 : 1;
+    return x->idx < y->idx ? -1 : (x->idx > y->idx); /* stable */
+}
+
+void orc_crossover(size_t n, size_t parents, const uint64_t* parent_masks,
+                   const uint32_t* parent_weights, uint64_t* child_masks, uint32_t* child_weights) {
+    const size_t mw = (n + 63) / 64, pool = parents * n;
+    orc_pool_entry* e = (orc_pool_entry*)malloc(pool * sizeof(orc_pool_entry));
+    for (size_t q = 0; q < pool; ++q) {
+        uint32_t pc = 0;
+        for (size_t w = 0; w < mw; ++w)
+            pc += popc64(parent_masks[q * mw + w]);
+        e[q].weight = parent_weights[q];
+        e[q].pc = pc;
+        e[q].idx = q;
+    }
+    qsort(e, pool, sizeof(orc_pool_entry), pool_cmp);
+    uint64_t* basis = (uint64_t*)calloc(n * mw, sizeof(uint64_t));
+    unsigned char* used = (unsigned char*)calloc(n, 1);
+    uint64_t* tmp = (uint64_t*)malloc(mw * sizeof(uint64_t));
+    uint64_t* unit = (uint64_t*)malloc(mw * sizeof(uint64_t));
+    size_t nchild = 0;
+    for (size_t q = 0; q < pool && nchild < n; ++q)
+        if (pivot_try_insert(basis, used, parent_masks + e[q].idx * mw, mw, tmp)) {
+            memcpy(child_masks + nchild * mw, parent_masks + e[q].idx * mw, mw * sizeof(uint64_t));
+            child_weights[nchild++] = parent_weights[e[q].idx];
+        }
+    for (size_t i = 0; i < n && nchild < n; ++i) {
+        memset(unit, 0, mw * sizeof(uint64_t));
+        unit[i / 64] = (uint64_t)1 << (i % 64);
+        if (pivot_try_insert(basis, used, unit, mw, tmp)) {
+            memcpy(child_masks + nchild * mw, unit, mw * sizeof(uint64_t));
+            child_weights[nchild++] = 1; /* Candidate(unit_mask, 1) */
+        }
+    }
+    free(unit);
+    free(tmp);
+    free(used);
+    free(basis);
+    free(e);
+}
+
+/* ---- One GeneticAlgorithm run (src/ga/genetic_algorithm_lifecycle.cpp:16-200,
+ * genetic_algorithm_population.cpp:10-83, genetic_algorithm_operators.cpp:15-192,
+ * genetic_algorithm_core.cpp:10-41). ---- */
+typedef struct {
+    const uint64_t* words;
+    size_t stride, cols, n, mw, P;
+    const size_t* win;
+    const orc_ga_config* cfg;
+    uint64_t rng;
+    double rate;
+} orc_ga_ctx;
+
+static uint64_t ind_fitness(const uint32_t* w, size_t n) {
+    uint64_t s = 0;
+    for (size_t i = 0; i < n; ++i)
+        s += w[i];
+    return s;
+}
+
+static uint32_t row_popcount(const orc_ga_ctx* g, size_t r) {
+    const size_t wpr = (g->cols + 63) / 64;
+    const uint64_t tail = tail_mask_for_cols(g->cols);
+    uint32_t s = 0;
+    for (size_t w = 0; w < wpr; ++w) {
+        uint64_t v = g->words[g->win[r] * g->stride + w];
+        if (w + 1 == wpr)
+            v &= tail;
+        s += popc64(v);
+    }
+    return s;
+}
+
+static void make_identity(const orc_ga_ctx* g, uint64_t* m, uint32_t* w) {
+    memset(m, 0, g->n * g->mw * sizeof(uint64_t));
+    for (size_t i = 0; i < g->n; ++i) {
+        m[i * g->mw + i / 64] = (uint64_t)1 << (i % 64);
+        w[i] = row_popcount(g, i);
+    }
+}
+
+static void make_random(orc_ga_ctx* g, uint64_t* m, uint32_t* w) {
+    make_identity(g, m, w);
+    for (size_t k = 0; k < g->n * 3; ++k) {
+        const size_t i = xs_index(&g->rng, g->n);
+        const size_t j = xs_index(&g->rng, g->n);
+        if (i == j)
+            continue;
+        for (size_t q = 0; q < g->mw; ++q)
+            m[i * g->mw + q] ^= m[j * g->mw + q];
+    }
+    for (size_t i = 0; i < g->n; ++i)
+        w[i] = orc_eval_cand_weight(g->words, g->stride, g->cols, g->win, g->n, m + i * g->mw,
+                                    g->mw);
+}
+
+static void make_heuristic(const orc_ga_ctx* g, uint64_t* m, uint32_t* w) {
+    make_identity(g, m, w);
+    const size_t n = g->n, mw = g->mw;
+    if (n < 2)
+        return;
+    size_t* order = (size_t*)malloc(n * sizeof(size_t));
+    for (size_t i = 0; i < n; ++i)
+        order[i] = i;
+    for (size_t a = 1; a < n; ++a) { /* stable insertion sort, descending weight */
+        const size_t v = order[a];
+        size_t b = a;
+        while (b > 0 && w[order[b - 1]] < w[v]) {
+            order[b] = order[b - 1];
+            --b;
+        }
+        order[b] = v;
+    }
+    const size_t probes = n < 5 ? n : 5;
+    for (size_t pos = 0; pos < probes; ++pos) {
+        const size_t i = order[pos];
+        uint32_t cur = w[i];
+        for (size_t j = 0; j < n; ++j) {
+            if (i == j)
+                continue;
+            for (size_t q = 0; q < mw; ++q)
+                m[i * mw + q] ^= m[j * mw + q];
+            const uint32_t cw =
+                orc_eval_cand_weight(g->words, g->stride, g->cols, g->win, n, m + i * mw, mw);
+            if (cw < cur) {
+                w[i] = cw;
+                cur = cw;
+                break;
+            }
+            for (size_t q = 0; q < mw; ++q)
+                m[i * mw + q] ^= m[j * mw + q];
+        }
+    }
+    free(order);
+}
+
+typedef struct {
+    uint64_t fit;
+    size_t idx;
+} orc_rank;
+
+static int rank_cmp(const void* a, const void* b) {
+    const orc_rank* x = (const orc_rank*)a;
+    const orc_rank* y = (const orc_rank*)b;
+    if (x->fit != y->fit)
+        return x->fit < y->fit ? -1 : 1;
+    return x->idx < y->idx ? -1 : (x->idx > y->idx);
+}
+
+static int should_stop(const orc_ga_config* c, uint64_t gens, uint64_t stale, uint64_t best) {
+    if ((c->flags & 1u) && gens >= c->max_generations)
+        return 1;
+    if ((c->flags & 2u) && stale >= c->max_stale_generations)
+        return 1;
+    if ((c->flags & 4u) && best <= c->target_total_weight)
+        return 1;
+    return 0;
+}
+
+long orc_ga_run(const uint64_t* words, size_t stride, size_t cols, const size_t* win, size_t n,
+                const orc_ga_config* cfg, uint64_t seed, uint64_t max_steps, uint64_t* scores,
+                uint64_t* best_masks, uint32_t* best_weights) {
+    orc_ga_ctx g;
+    g.words = words;
+    g.stride = stride;
+    g.cols = cols;
+    g.win = win;
+    g.n = n;
+    g.mw = (n + 63) / 64;
+    g.P = cfg->population_size;
+    g.cfg = cfg;
+    g.rng = orc_xs_seed(seed);
+    g.rate = cfg->mutation_rate;
+    if (n == 0 || cols == 0 || g.P == 0)
+        return ORC_EINVAL;
+    const size_t P = g.P, mw = g.mw, isz = n * mw;
+    uint64_t* pm = (uint64_t*)malloc(P * isz * sizeof(uint64_t));
+    uint32_t* pw = (uint32_t*)malloc(P * n * sizeof(uint32_t));
+    uint64_t* nm = (uint64_t*)malloc(P * isz * sizeof(uint64_t));
+    uint32_t* nw = (uint32_t*)malloc(P * n * sizeof(uint32_t));
+    uint64_t* fit = (uint64_t*)malloc(P * sizeof(uint64_t));
+    orc_rank* rk = (orc_rank*)malloc(P * sizeof(orc_rank));
+    const size_t np = cfg->num_parents ? cfg->num_parents : 1;
+    uint64_t* par_m = (uint64_t*)malloc(np * isz * sizeof(uint64_t));
+    uint32_t* par_w = (uint32_t*)malloc(np * n * sizeof(uint32_t));
+    uint64_t* child_m = (uint64_t*)malloc(isz * sizeof(uint64_t));
+    uint32_t* child_w = (uint32_t*)malloc(n * sizeof(uint32_t));
+
+    /* initialize */
+    make_identity(&g, pm, pw);
+    size_t heur = P / 4 < P - 1 ? P / 4 : P - 1;
+    size_t filled = 1;
+    for (size_t i = 0; i < heur; ++i, ++filled)
+        make_heuristic(&g, pm + filled * isz, pw + filled * n);
+    for (; filled < P; ++filled)
+        make_random(&g, pm + filled * isz, pw + filled * n);
+    for (size_t i = 0; i < P; ++i)
+        fit[i] = ind_fitness(pw + i * n, n);
+    size_t bi = 0;
+    for (size_t i = 1; i < P; ++i)
+        if (fit[i] < fit[bi])
+            bi = i;
+    uint64_t best = fit[bi];
+    memcpy(best_masks, pm + bi * isz, isz * sizeof(uint64_t));
+    memcpy(best_weights, pw + bi * n, n * sizeof(uint32_t));
+    uint64_t gens = 0, stale = 0, no_imp = 0, cat = 0;
+    scores[0] = best;
+    int done = should_stop(cfg, gens, stale, best);
+    long steps = 0;
+    while (!done && (uint64_t)steps < max_steps) {
+        /* adapt_mutation_rate */
+        if (no_imp > 10)
+            g.rate = g.rate * 1.5 < 0.8 ? g.rate * 1.5 : 0.8;
+        else if (no_imp > 5)
+            g.rate = g.rate * 1.3 < 0.6 ? g.rate * 1.3 : 0.6;
+        else
+            g.rate = g.rate * 0.95 > 0.3 ? g.rate * 0.95 : 0.3;
+        for (size_t i = 0; i < P; ++i) {
+            rk[i].fit = fit[i];
+            rk[i].idx = i;
+        }
+        qsort(rk, P, sizeof(orc_rank), rank_cmp);
+        size_t out = 0;
+        for (size_t e = 0; e < cfg->elite_count && e < P; ++e, ++out) {
+            memcpy(nm + out * isz, pm + rk[e].idx * isz, isz * sizeof(uint64_t));
+            memcpy(nw + out * n, pw + rk[e].idx * n, n * sizeof(uint32_t));
+        }
+        while (out < P) {
+            if (no_imp > 15 && xs_unit(&g.rng) < 0.2) {
+                make_random(&g, nm + out * isz, nw + out * n);
+                ++out;
+                continue;
+            }
+            for (size_t p = 0; p < np; ++p) { /* tournament_selection */
+                size_t b = xs_index(&g.rng, P);
+                for (size_t t = 1; t < cfg->tournament_size; ++t) {
+                    const size_t c = xs_index(&g.rng, P);
+                    if (fit[c] < fit[b])
+                        b = c;
+                }
+                memcpy(par_m + p * isz, pm + b * isz, isz * sizeof(uint64_t));
+                memcpy(par_w + p * n, pw + b * n, n * sizeof(uint32_t));
+            }
+            orc_crossover(n, np, par_m, par_w, child_m, child_w);
+            for (size_t o = 0; o < cfg->num_offspring && out < P; ++o, ++out) {
+                uint64_t* cm = nm + out * isz;
+                uint32_t* cw = nw + out * n;
+                memcpy(cm, child_m, isz * sizeof(uint64_t));
+                memcpy(cw, child_w, n * sizeof(uint32_t));
+                orc_mutate(words, stride, cols, win, n, cm, cw, mw, g.rate, &g.rng);
+                if (gens % 3 == 0)
+                    orc_local_improvement(words, stride, cols, win, n, cm, cw, mw);
+            }
+        }
+        uint64_t* tm = pm;
+        pm = nm;
+        nm = tm;
+        uint32_t* tw = pw;
+        pw = nw;
+        nw = tw;
+        for (size_t i = 0; i < P; ++i)
+            fit[i] = ind_fitness(pw + i * n, n);
+        ++gens;
+        bi = 0;
+        for (size_t i = 1; i < P; ++i)
+            if (fit[i] < fit[bi])
+                bi = i;
+        if (fit[bi] < best) {
+            best = fit[bi];
+            memcpy(best_masks, pm + bi * isz, isz * sizeof(uint64_t));
+            memcpy(best_weights, pw + bi * n, n * sizeof(uint32_t));
+            stale = 0;
+            no_imp = 0;
+            cat = 0;
+        } else {
+            ++stale;
+            ++no_imp;
+            ++cat;
+        }
+        if (cfg->enable_catastrophe && cat == cfg->catastrophe_threshold) {
+            /* catastrophe(): ranked survivors, then make_random */
+            const size_t sv = (size_t)((double)P * cfg->catastrophe_survival_rate);
+            for (size_t i = 0; i < P; ++i) {
+                rk[i].fit = fit[i];
+                rk[i].idx = i;
+            }
+            qsort(rk, P, sizeof(orc_rank), rank_cmp);
+            size_t o = 0;
+            for (; o < sv && o < P; ++o) {
+                memcpy(nm + o * isz, pm + rk[o].idx * isz, isz * sizeof(uint64_t));
+                memcpy(nw + o * n, pw + rk[o].idx * n, n * sizeof(uint32_t));
+            }
+            for (; o < P; ++o)
+                make_random(&g, nm + o * isz, nw + o * n);
+            tm = pm;
+            pm = nm;
+            nm = tm;
+            tw = pw;
+            pw = nw;
+            nw = tw;
+            for (size_t i = 0; i < P; ++i)
+                fit[i] = ind_fitness(pw + i * n, n);
+            cat = 0;
+            bi = 0;
+            for (size_t i = 1; i < P; ++i)
+                if (fit[i] < fit[bi])
+                    bi = i;
+            if (fit[bi] < best) {
+                best = fit[bi];
+                memcpy(best_masks, pm + bi * isz, isz * sizeof(uint64_t));
+                memcpy(best_weights, pw + bi * n, n * sizeof(uint32_t));
+            }
+        }
+        done = should_stop(cfg, gens, stale, best);
+        ++steps;
+        scores[steps] = best;
+    }
+    free(child_w);
+    free(child_m);
+    free(par_w);
+    free(par_m);
+    free(rk);
+    free(fit);
+    free(nw);
+    free(nm);
+    free(pw);
+    free(pm);
+    return steps;
+}

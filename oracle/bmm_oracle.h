@@ -99,6 +99,30 @@ void orc_mutate(const uint64_t* words, size_t stride, size_t cols, const size_t*
 void orc_local_improvement(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
                            size_t n, uint64_t* masks, uint32_t* weights, size_t mw);
 
+/* GeneticAlgorithm::crossover: parents individuals of n candidates laid out
+ * one after another; the child's masks/weights (unit padding weighs 1). */
+void orc_crossover(size_t n, size_t parents, const uint64_t* parent_masks,
+                   const uint32_t* parent_weights, uint64_t* child_masks,
+                   uint32_t* child_weights);
+
+/* GeneticAlgorithmConfig (include/bmmpy/ga/genetic_algorithm.hpp:17-29);
+ * flags: 1 max_generations, 2 max_stale_generations, 4 target_total_weight. */
+typedef struct orc_ga_config {
+    size_t population_size, elite_count, num_parents, num_offspring, tournament_size;
+    int enable_catastrophe;
+    size_t catastrophe_threshold;
+    double catastrophe_survival_rate, mutation_rate;
+    unsigned flags;
+    uint64_t max_generations, max_stale_generations, target_total_weight;
+} orc_ga_config;
+
+/* initialize() then step() until done() or max_steps steps.  scores[g] is
+ * best_score() after g steps (scores[0] after initialize); best_masks /
+ * best_weights receive best_individual().  Returns the number of steps. */
+long orc_ga_run(const uint64_t* words, size_t stride, size_t cols, const size_t* win, size_t n,
+                const orc_ga_config* cfg, uint64_t seed, uint64_t max_steps, uint64_t* scores,
+                uint64_t* best_masks, uint32_t* best_weights);
+
 #ifdef __cplusplus
 }
 #endif

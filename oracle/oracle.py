@@ -35,6 +35,33 @@ class OracleError(RuntimeError):
     pass
 
 
+class GaConfig(C.Structure):
+    """GeneticAlgorithmConfig as orc_ga_config / refh_ga_config (flags: 1
+    max_generations, 2 max_stale_generations, 4 target_total_weight)."""
+
+    _fields_ = [("population_size", C.c_size_t), ("elite_count", C.c_size_t),
+                ("num_parents", C.c_size_t), ("num_offspring", C.c_size_t),
+                ("tournament_size", C.c_size_t), ("enable_catastrophe", C.c_int),
+                ("catastrophe_threshold", C.c_size_t),
+                ("catastrophe_survival_rate", C.c_double), ("mutation_rate", C.c_double),
+                ("flags", C.c_uint), ("max_generations", C.c_uint64),
+                ("max_stale_generations", C.c_uint64), ("target_total_weight", C.c_uint64)]
+
+
+def ga_config(population_size=300, elite_count=3, num_parents=2, num_offspring=1,
+              tournament_size=3, enable_catastrophe=False, catastrophe_threshold=30,
+              catastrophe_survival_rate=0.2, mutation_rate=0.3, max_generations=None,
+              max_stale_generations=None, target_total_weight=None) -> GaConfig:
+    """Defaults of include/bmmpy/ga/genetic_algorithm.hpp:17-29."""
+    flags = ((1 if max_generations is not None else 0)
+             | (2 if max_stale_generations is not None else 0)
+             | (4 if target_total_weight is not None else 0))
+    return GaConfig(population_size, elite_count, num_parents, num_offspring, tournament_size,
+                    int(bool(enable_catastrophe)), catastrophe_threshold,
+                    catastrophe_survival_rate, mutation_rate, flags, max_generations or 0,
+                    max_stale_generations or 0, target_total_weight or 0)
+
+
 ERRORS = {-1: ValueError, -2: OverflowError, -3: IndexError, -4: RuntimeError, -5: RuntimeError}
 
 
@@ -69,6 +96,10 @@ def _load_port():
     lib.orc_eval_cand_weight.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p, _sz]
     lib.orc_mutate.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, _sz, C.c_double, _u64p]
     lib.orc_local_improvement.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, _sz]
+    lib.orc_crossover.argtypes = [_sz, _sz, _u64p, _u32p, _u64p, _u32p]
+    lib.orc_ga_run.restype = C.c_long
+    lib.orc_ga_run.argtypes = [_u64p, _sz, _sz, _szp, _sz, C.POINTER(GaConfig), C.c_uint64,
+                               C.c_uint64, _u64p, _u64p, _u32p]
     return lib
 
 
@@ -198,6 +229,32 @@ class Port(_Searches):
                                        len(win), _ptr(masks, _u64p), _ptr(weights, _u32p),
                                        masks.shape[1])
 
+    def crossover(self, parent_masks, parent_weights):
+        """parent_masks: (parents, n, mw) uint64; parent_weights: (parents, n)."""
+        pm = np.ascontiguousarray(parent_masks, dtype=np.uint64)
+        pw = np.ascontiguousarray(parent_weights, dtype=np.uint32)
+        np_, n, mw = pm.shape
+        cm = np.zeros((n, mw), np.uint64)
+        cw = np.zeros(n, np.uint32)
+        self.lib.orc_crossover(n, np_, _ptr(pm, _u64p), _ptr(pw, _u32p), _ptr(cm, _u64p),
+                               _ptr(cw, _u32p))
+        return cm, cw
+
+    def ga_run(self, m, cols, win, cfg: GaConfig, seed, max_steps):
+        """initialize() + step()s: (scores per step, best masks (n, mw), best weights)."""
+        win = self._win(win)
+        n = len(win)
+        mw = (n + 63) // 64
+        scores = np.zeros(max_steps + 1, np.uint64)
+        bm = np.zeros((n, mw), np.uint64)
+        bw = np.zeros(n, np.uint32)
+        g = self.lib.orc_ga_run(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp), n,
+                                C.byref(cfg), seed, max_steps, _ptr(scores, _u64p),
+                                _ptr(bm, _u64p), _ptr(bw, _u32p))
+        if g < 0:
+            raise ERRORS.get(g, OracleError)("oracle error")
+        return scores[: g + 1].tolist(), bm, bw
+
 
 class Ref(_Searches):
     """The reference library itself (oracle/_ref/libbmmref.so)."""
@@ -222,8 +279,8 @@ class Ref(_Searches):
         L.refh_target_best_fwht.restype = C.c_long
         L.refh_target_best_fwht.argtypes = [_u64p, _sz, _sz, _sz, _sz, _szp, _sz, _u64p, _u32p]
         L.refh_ga_run.restype = C.c_long
-        L.refh_ga_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_double,
-                                  C.c_uint64, _sz, C.c_uint64, _u64p, C.POINTER(C.c_double)]
+        L.refh_ga_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, C.POINTER(GaConfig),
+                                  C.c_uint64, _sz, _u64p, _u64p, _u32p, C.POINTER(C.c_double)]
         L.refh_island_run.restype = C.c_long
         L.refh_island_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_uint64,
                                       _sz, C.c_uint64, C.c_double, _u64p, C.POINTER(C.c_double)]
@@ -285,16 +342,21 @@ class Ref(_Searches):
             raise ERRORS.get(rc, OracleError)("reference error")
         return int(bm.value), int(bw.value)
 
-    def ga_run(self, m, cols, win, population, elite, tournament, rate, seed, gens, target=0):
+    def ga_run(self, m, cols, win, cfg: GaConfig, seed, max_steps):
+        """GeneticAlgorithm: (scores per step, best masks (n, mw), best weights, seconds)."""
         win = self._win(win)
-        scores = np.zeros(gens + 1, np.uint64)
+        n = len(win)
+        mw = (n + 63) // 64
+        scores = np.zeros(max_steps + 1, np.uint64)
+        bm = np.zeros((n, mw), np.uint64)
+        bw = np.zeros(n, np.uint32)
         secs = C.c_double(0)
         g = self.lib.refh_ga_run(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], _ptr(win, _szp),
-                                 len(win), population, elite, tournament, rate, seed, gens, target,
-                                 _ptr(scores, _u64p), C.byref(secs))
+                                 n, C.byref(cfg), seed, max_steps, _ptr(scores, _u64p),
+                                 _ptr(bm, _u64p), _ptr(bw, _u32p), C.byref(secs))
         if g < 0:
             raise ERRORS.get(g, OracleError)("reference error")
-        return scores[: g + 1].tolist(), secs.value
+        return scores[: g + 1].tolist(), bm, bw, secs.value
 
     def island_run(self, m, cols, win, islands, population, interval, seed, max_gens, target,
                    cap_seconds):

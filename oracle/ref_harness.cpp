@@ -195,34 +195,64 @@ long refh_target_best_fwht(const std::uint64_t* words, std::size_t rows, std::si
 
 // Single-island bmmpy::ga::GeneticAlgorithm run; best_score after
 // initialize() and after each generation is written to scores[0..gens].
+// GeneticAlgorithmConfig fields, laid out like orc_ga_config (bmm_oracle.h);
+// flags: 1 max_generations, 2 max_stale_generations, 4 target_total_weight.
+struct refh_ga_config {
+    std::size_t population_size, elite_count, num_parents, num_offspring, tournament_size;
+    int enable_catastrophe;
+    std::size_t catastrophe_threshold;
+    double catastrophe_survival_rate, mutation_rate;
+    unsigned flags;
+    std::uint64_t max_generations, max_stale_generations, target_total_weight;
+};
+
+// The reference bmmpy::ga::GeneticAlgorithm: initialize(), then step() until
+// done() or max_steps.  scores[g] = best_score() after g steps; best_masks
+// (n * ceil(n/64) words) / best_weights receive best_individual().  Returns
+// the number of steps; seconds receives the wall time.
 long refh_ga_run(const std::uint64_t* words, std::size_t rows, std::size_t cols,
                  std::size_t stride, const std::size_t* win, std::size_t t,
-                 std::size_t population, std::size_t elite, std::size_t tournament,
-                 double mutation_rate, std::uint64_t seed, std::size_t gens,
-                 std::uint64_t target_weight, std::uint64_t* scores, double* seconds) {
+                 const refh_ga_config* c, std::uint64_t seed, std::size_t max_steps,
+                 std::uint64_t* scores, std::uint64_t* best_masks, std::uint32_t* best_weights,
+                 double* seconds) {
     return guarded([&] {
         const auto m = make_matrix(words, rows, cols, stride);
         const auto w = m.row_window(to_rows(win, t));
         bmmpy::ga::GeneticAlgorithmConfig cfg;
-        cfg.population_size = population;
-        cfg.elite_count = elite;
-        cfg.tournament_size = tournament;
-        cfg.mutation_rate = mutation_rate;
+        cfg.population_size = c->population_size;
+        cfg.elite_count = c->elite_count;
+        cfg.num_parents = c->num_parents;
+        cfg.num_offspring = c->num_offspring;
+        cfg.tournament_size = c->tournament_size;
+        cfg.enable_catastrophe = c->enable_catastrophe != 0;
+        cfg.catastrophe_threshold = c->catastrophe_threshold;
+        cfg.catastrophe_survival_rate = c->catastrophe_survival_rate;
+        cfg.mutation_rate = c->mutation_rate;
         cfg.seed = seed;
-        cfg.stop.max_generations = gens;
-        if (target_weight != 0)
-            cfg.stop.target_total_weight = target_weight;
+        if (c->flags & 1u)
+            cfg.stop.max_generations = c->max_generations;
+        if (c->flags & 2u)
+            cfg.stop.max_stale_generations = c->max_stale_generations;
+        if (c->flags & 4u)
+            cfg.stop.target_total_weight = c->target_total_weight;
         bmmpy::ga::GeneticAlgorithm ga(cfg);
         const auto t0 = std::chrono::steady_clock::now();
         ga.initialize(w);
         scores[0] = ga.best_score();
         std::size_t g = 0;
-        while (!ga.done()) {
+        while (!ga.done() && g < max_steps) {
             ga.step();
             ++g;
             scores[g] = ga.best_score();
         }
         *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        const auto best = ga.best_individual();
+        const std::size_t mw = (t + 63) / 64;
+        for (std::size_t i = 0; i < best.size() && i < t; ++i) {
+            for (std::size_t q = 0; q < mw; ++q)
+                best_masks[i * mw + q] = q < best[i].mask.size() ? best[i].mask[q] : 0;
+            best_weights[i] = best[i].weight;
+        }
         return static_cast<long>(g);
     });
 }

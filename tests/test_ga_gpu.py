@@ -1,0 +1,296 @@
+"""GPU parity of the genetic algorithm.
+
+* Operators (eval_cand_weight, mutate, local_improvement, crossover) through
+  the C ABI against the C oracle on seeded inputs, bit for bit, including the
+  generator state after mutation.
+* Whole single-island runs against the oracle's GeneticAlgorithm
+  restatement: best score after every generation and the final best
+  individual, over configurations that exercise restarts, several parents and
+  offspring, catastrophes and every stop criterion.
+* The reference's own Python GA tests (tests/python/test_ga_api.py) against
+  this package, and island-model invariants.
+"""
+
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import bmmpy_b200 as bmm
+from bmmpy_b200 import _native as N
+from bmmpy_b200.matrix import BitMatrix
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+def _instance(rows, cols, p, seed, scrambles):
+    words, planted = O.port().gen_instance(rows, cols, p, seed, scrambles)
+    m = BitMatrix(rows, cols)
+    m.words[:] = words[:, : m.stride_words]
+    return words, m, planted
+
+
+def _random_individual(n, rng, pairs):
+    mw = (n + 63) // 64
+    masks = np.zeros((n, mw), np.uint64)
+    for i in range(n):
+        masks[i, i // 64] = np.uint64(1 << (i % 64))
+    for _ in range(pairs):
+        i, j = rng.integers(0, n, 2)
+        if i != j:
+            masks[i] ^= masks[j]
+    return masks
+
+
+def _win_args(words, win):
+    w = np.ascontiguousarray(words)
+    wi = np.ascontiguousarray(np.asarray(win, dtype=np.uintp))
+    return w, wi
+
+
+SHAPES = [(1, 70), (2, 64), (17, 100), (40, 512), (64, 130), (65, 200), (130, 257), (256, 1024)]
+
+
+@pytest.mark.parametrize("n,cols", SHAPES)
+def test_eval_matches_oracle(n, cols):
+    words, m, _ = _instance(n + 3, cols, 0.3, 11 + n, 2 * n)
+    rng = np.random.default_rng(n * 7 + cols)
+    win = list(rng.permutation(n + 3)[:n])
+    mw = (n + 63) // 64
+    masks = rng.integers(0, 2**63, size=(50, mw), dtype=np.uint64)
+    if n % 64:
+        masks[:, -1] &= np.uint64((1 << (n % 64)) - 1)
+    w, wi = _win_args(words, win)
+    out = np.zeros(50, np.uint32)
+    N.check(N.lib().bmm_ga_eval(N.u64p(w), w.shape[1], cols, N.szp(wi), n, N.u64p(masks), 50,
+                                N.u32p(out)))
+    want = [O.port().eval_cand_weight(words, cols, win, masks[c]) for c in range(50)]
+    assert out.tolist() == want
+
+
+@pytest.mark.parametrize("n,cols", SHAPES)
+@pytest.mark.parametrize("rate", [0.3, 0.8, 2.5])
+def test_mutate_matches_oracle(n, cols, rate):
+    words, m, _ = _instance(n, cols, 0.2, 5 + n, n)
+    rng = np.random.default_rng(n + cols)
+    masks = _random_individual(n, rng, 3 * n)
+    weights = rng.integers(0, 1000, n).astype(np.uint32)
+    win = list(range(n))
+    state = 0x1234567 + n
+    want_m, want_w = masks.copy(), weights.copy()
+    want_state = O.port().mutate(words, cols, win, want_m, want_w, rate, state)
+    w, wi = _win_args(words, win)
+    got_m, got_w = masks.copy(), weights.copy()
+    st = C.c_uint64(state)
+    N.check(N.lib().bmm_ga_mutate(N.u64p(w), w.shape[1], cols, N.szp(wi), n, N.u64p(got_m),
+                                  N.u32p(got_w), rate, C.byref(st)))
+    assert np.array_equal(got_m, want_m)
+    assert np.array_equal(got_w, want_w)
+    assert st.value == (want_state if n >= 2 else state)
+
+
+@pytest.mark.parametrize("n,cols", SHAPES)
+def test_local_improvement_matches_oracle(n, cols):
+    words, m, _ = _instance(n, cols, 0.05, 21 + n, 4 * n)
+    rng = np.random.default_rng(3 * n + cols)
+    masks = _random_individual(n, rng, n)
+    weights = np.zeros(n, np.uint32)
+    win = list(range(n))
+    want_m, want_w = masks.copy(), weights.copy()
+    O.port().local_improvement(words, cols, win, want_m, want_w)
+    w, wi = _win_args(words, win)
+    got_m, got_w = masks.copy(), weights.copy()
+    N.check(N.lib().bmm_ga_local_improve(N.u64p(w), w.shape[1], cols, N.szp(wi), n,
+                                         N.u64p(got_m), N.u32p(got_w)))
+    assert np.array_equal(got_m, want_m)
+    if n >= 2:
+        assert np.array_equal(got_w, want_w)
+
+
+@pytest.mark.parametrize("n", [1, 5, 63, 64, 100, 256])
+@pytest.mark.parametrize("parents", [1, 2, 3, 4])
+def test_crossover_matches_oracle(n, parents):
+    rng = np.random.default_rng(n * 10 + parents)
+    pm = np.stack([_random_individual(n, rng, 2 * n) for _ in range(parents)])
+    pw = rng.integers(0, 6, size=(parents, n)).astype(np.uint32)  # many ties
+    if n > 3:  # rank-deficient parents exercise the unit padding
+        pm[:, 1] = pm[:, 0]
+        pm[:, 2] = 0
+    want_m, want_w = O.port().crossover(pm, pw)
+    got_m = np.zeros_like(want_m)
+    got_w = np.zeros_like(want_w)
+    pmc = np.ascontiguousarray(pm)
+    pwc = np.ascontiguousarray(pw)
+    N.check(N.lib().bmm_ga_crossover(n, parents, N.u64p(pmc), N.u32p(pwc), N.u64p(got_m),
+                                     N.u32p(got_w)))
+    assert np.array_equal(got_m, want_m)
+    assert np.array_equal(got_w, want_w)
+
+
+TRAJECTORIES = [
+    # rows, cols, p, inst seed, scrambles, ga kwargs, steps
+    (16, 200, 0.2, 3, 40, dict(population_size=20, max_generations=40), 40),
+    (24, 130, 0.1, 5, 100, dict(population_size=32, max_generations=30), 30),
+    (40, 512, 0.05, 9, 160, dict(population_size=24, num_parents=3, num_offspring=2,
+                                  elite_count=2, max_generations=20), 20),
+    (20, 100, 0.3, 1, 50, dict(population_size=16, enable_catastrophe=True,
+                                catastrophe_threshold=4, catastrophe_survival_rate=0.25,
+                                tournament_size=2, max_generations=60), 60),
+    (70, 300, 0.02, 4, 300, dict(population_size=12, max_generations=12), 12),
+    (33, 1000, 0.1, 8, 120, dict(population_size=40, max_stale_generations=6,
+                                 max_generations=200), 200),
+    (12, 64, 0.4, 2, 30, dict(population_size=10, target_total_weight=150,
+                               max_generations=300), 300),
+    (130, 257, 0.03, 6, 500, dict(population_size=16, elite_count=0, tournament_size=5,
+                                  mutation_rate=0.6, max_generations=9), 9),
+]
+
+
+@pytest.mark.parametrize("case", TRAJECTORIES, ids=lambda c: f"{c[0]}x{c[1]}")
+def test_single_island_trajectory_matches_oracle(case):
+    rows, cols, p, iseed, scr, kw, steps = case
+    words, m, _ = _instance(rows, cols, p, iseed, scr)
+    win = list(range(rows))
+    cfg = O.ga_config(**kw)
+    want_scores, want_m, want_w = O.port().ga_run(words, cols, win, cfg, iseed + 11, steps)
+    ga = bmm.GeneticAlgorithm(seed=iseed + 11, **kw)
+    ga.initialize(m.row_window(win))
+    got = [ga.best_score()]
+    while not ga.done() and len(got) <= steps:
+        ga.step()
+        got.append(ga.best_score())
+    assert got == want_scores
+    best = ga.best_individual()
+    assert [c.mask for c in best] == want_m.tolist()
+    assert [c.weight for c in best] == want_w.tolist()
+    assert ga.best_score() == sum(c.weight for c in best)
+    st = ga.stats()
+    assert st.generations == len(want_scores) - 1 == ga.generation()
+    assert st.evaluations == kw["population_size"] * (st.generations + 1)
+
+
+def _ga_matrix():
+    return bmm.matrix_from_rows(["11001000", "01100100", "00100110", "10010001"])
+
+
+def _spec(island_id, interval):
+    mig = bmm.MigrationPolicy()
+    mig.interval_generations = interval
+    mig.export_count = 1
+    mig.import_count = 1
+    spec = bmm.IslandSpec()
+    spec.island_id = island_id
+    spec.migration = mig
+    return spec
+
+
+def _native_cfg(seed):
+    c = bmm.ga.GeneticAlgorithmConfig()
+    c.population_size = 12
+    c.elite_count = 2
+    c.tournament_size = 2
+    c.mutation_rate = 0.25
+    c.num_parents = 2
+    c.num_offspring = 1
+    c.enable_catastrophe = True
+    c.catastrophe_threshold = 2
+    c.catastrophe_survival_rate = 0.5
+    c.stop.max_generations = 4
+    c.stop.max_stale_generations = 4
+    c.seed = seed
+    return c
+
+
+def test_reference_stepwise_wrapper():
+    ga = bmm.GeneticAlgorithm(population_size=16, elite_count=2, tournament_size=2,
+                              mutation_rate=0.3, max_generations=4, max_stale_generations=4,
+                              seed=7, num_parents=2, num_offspring=1, enable_catastrophe=True,
+                              catastrophe_threshold=2, catastrophe_survival_rate=0.5)
+    ga.initialize(_ga_matrix().row_window([0, 1, 2, 3]))
+    while not ga.done():
+        ga.step()
+    individual = ga.best_individual()
+    stats = ga.stats()
+    assert ga.name() == "ga"
+    assert len(individual) == 4
+    assert ga.best_score() == sum(c.weight for c in individual)
+    assert stats.generations == ga.generation()
+    assert stats.evaluations > 0
+    assert stats.seed == 7
+
+
+def test_reference_island_model_wrapper():
+    window = _ga_matrix().row_window([0, 1, 2, 3])
+    model = bmm.IslandModel(islands=[_spec(0, 4), _spec(1, 6)],
+                            ga_configs=[_native_cfg(11), _native_cfg(19)],
+                            channel_capacity=32, overflow_policy="drop_oldest")
+    best = model.run_to_completion(window)
+    snap = model.snapshot()
+    assert model.name() == "island_model"
+    assert len(best) == 4
+    assert snap.island_count == 2 and len(snap.islands) == 2
+    assert snap.best_score == sum(c.weight for c in best)
+    assert not snap.running
+
+
+def _gf2_rank(masks):
+    rows = [int.from_bytes(np.asarray(r, dtype=np.uint64).tobytes(), "little") for r in masks]
+    rank = 0
+    while rows:
+        piv = max(rows)
+        if piv == 0:
+            break
+        rows.remove(piv)
+        hb = piv.bit_length() - 1
+        rows = [r ^ piv if (r >> hb) & 1 else r for r in rows]
+        rank += 1
+    return rank
+
+
+def test_island_ring_invariants():
+    words, m, planted = _instance(48, 700, 0.03, 13, 200)
+    win = list(range(48))
+    islands = [_spec(i, 3) for i in range(6)]
+    model = bmm.IslandModel(islands=islands, population_size=24, max_generations=30, seed=5)
+    best = model.run_to_completion(m.row_window(win))
+    snap = model.snapshot()
+    assert snap.best_score == sum(c.weight for c in best)
+    assert snap.total_generations == 6 * 30
+    assert all(i.finished for i in snap.islands)
+    for isl in snap.islands:  # each island's best is a basis with exact weights
+        masks = np.array([c.mask for c in isl.best_individual], dtype=np.uint64)
+        assert _gf2_rank(masks) == 48
+        weights = np.zeros(48, np.uint32)
+        w, wi = _win_args(words, win)
+        N.check(N.lib().bmm_ga_eval(N.u64p(w), w.shape[1], 700, N.szp(wi), 48, N.u64p(masks),
+                                    48, N.u32p(weights)))
+        assert weights.tolist() == [c.weight for c in isl.best_individual]
+        assert isl.best_score == int(weights.sum())
+    # deterministic for a seed
+    again = bmm.IslandModel(islands=islands, population_size=24, max_generations=30, seed=5)
+    again.run_to_completion(m.row_window(win))
+    assert again.snapshot().best_score == snap.best_score
+    # islands without migration are independent single-island runs
+    solo = bmm.IslandModel(islands=[_spec(i, 0) for i in range(3)], population_size=24,
+                           max_generations=30, seed=5)
+    solo.run_to_completion(m.row_window(win))
+    for i, isl in enumerate(solo.snapshot().islands):
+        ga = bmm.GeneticAlgorithm(population_size=24, max_generations=30, seed=5 + i)
+        ga.optimize(m.row_window(win))
+        assert isl.best_score == ga.best_score()
+
+
+def test_invalid_arguments():
+    m = _ga_matrix()
+    with pytest.raises(ValueError):
+        bmm.GeneticAlgorithm(population_size=0).initialize(m.row_window([0, 1]))
+    with pytest.raises(ValueError):
+        bmm.GeneticAlgorithm().initialize(m.row_window([]))
+    with pytest.raises(ValueError):
+        bmm.IslandModel(islands=[])
+    with pytest.raises(ValueError):
+        bmm.IslandModel(islands=[_spec(0, 1)], overflow_policy="bogus")
+    big = BitMatrix(300, 64)
+    with pytest.raises(ValueError):
+        bmm.GeneticAlgorithm().initialize(big.row_window(list(range(257))))
