@@ -25,6 +25,23 @@ C2 = dict(rows=40, cols=4096, p=0.3, seed=1, k=24)
 C3 = dict(rows=512, cols=65536, p=0.02, seed=2, scrambles=2000, window=32, golden_windows=2)
 # C4: 4096 uneven planted instances (seeds 1000..5095)
 C4 = dict(count=4096, seed0=1000, p=0.05)
+# C5: GA on a planted 256x8192 instance (p=0.01, seed 7, 5000 scrambles)
+C5 = dict(rows=256, cols=8192, p=0.01, seed=7, scrambles=5000)
+
+# Single-island GeneticAlgorithm runs pinned by the reference:
+# (rows, cols, p, instance seed, scrambles, GA keyword arguments, steps, GA seed)
+GA_CASES = [
+    (16, 200, 0.2, 3, 40, dict(population_size=20, max_generations=30), 30, 14),
+    (40, 512, 0.05, 9, 160, dict(population_size=24, num_parents=3, num_offspring=2,
+                                  elite_count=2, max_generations=15), 15, 20),
+    (20, 100, 0.3, 1, 50, dict(population_size=16, enable_catastrophe=True,
+                                catastrophe_threshold=4, catastrophe_survival_rate=0.25,
+                                tournament_size=2, max_generations=50), 50, 12),
+    (12, 64, 0.4, 2, 30, dict(population_size=10, target_total_weight=150,
+                               max_generations=300), 300, 13),
+    (C5["rows"], C5["cols"], C5["p"], C5["seed"], C5["scrambles"],
+     dict(population_size=12, max_generations=4), 4, 77),
+]
 
 
 def stride_for(cols: int) -> int:

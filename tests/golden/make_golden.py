@@ -15,8 +15,10 @@ library (oracle/_ref/libbmmref.so), called through oracle/ref_harness.cpp:
 * ``workloads.npz`` -- per-target results for the seeded synthetic workloads
   (the C1 64x256 FWHT case, the C2 40x4096 Gray-code case at full size, the
   C4 batch as per-instance checksums) and MITM top-k lists for windows of the
-  C3 planted instance.  Matrices are regenerated from their seeds at test
-  time (xorshift64 Bernoulli fill, see oracle/bmm_oracle.c:orc_gen_instance).
+  C3 planted instance, and single-island GeneticAlgorithm trajectories (best
+  score after every step, final best individual) for the GA_CASES of
+  fixtures.py.  Matrices are regenerated from their seeds at test time
+  (xorshift64 Bernoulli fill, see oracle/bmm_oracle.c:orc_gen_instance).
 """
 
 from __future__ import annotations
@@ -36,10 +38,12 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from oracle.oracle import port, ref  # noqa: E402
+from oracle.oracle import ga_config  # noqa: E402
 from tests.golden.fixtures import (  # noqa: E402
     C1,
     C2,
     C3,
+    GA_CASES,
     batch_instance,
     cuda_equivalence_matrix,
     matrix_from_rows,
@@ -100,7 +104,7 @@ def per_target(R, m, cols, rows, k, offset=1):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-slow", action="store_true")
-    ap.add_argument("--only", default="", help="comma list of c1,c2,c3,c4,ka to regenerate; "
+    ap.add_argument("--only", default="", help="comma list of c1,c2,c3,c4,ga,ka to regenerate; "
                     "the other entries of workloads.npz are kept")
     args = ap.parse_args()
     only = set(filter(None, args.only.split(",")))
@@ -129,6 +133,8 @@ def main():
         c4(R, P, arrays)
     if want("c3") and not args.skip_slow:
         c3(R, P, arrays)
+    if want("ga"):
+        ga(R, P, arrays)
     np.savez_compressed(npz, **arrays)
     print("workloads.npz written")
 
@@ -182,6 +188,18 @@ def c3(R, P, arrays):
         print("  C3 window", j, time.time() - t0)
     arrays["c3_top64"] = np.stack(tops, 0)
     print("C3 done", time.time() - t0)
+
+
+def ga(R, P, arrays):
+    t0 = time.time()
+    for i, (rows, cols, p, iseed, scr, kw, steps, gseed) in enumerate(GA_CASES):
+        m, _ = P.gen_instance(rows, cols, p, iseed, scr)
+        scores, bm, bw, secs = R.ga_run(m, cols, list(range(rows)), ga_config(**kw), gseed, steps)
+        arrays[f"ga{i}_scores"] = np.array(scores, np.uint64)
+        arrays[f"ga{i}_masks"] = bm
+        arrays[f"ga{i}_weights"] = bw
+        print(f"  GA case {i}: {len(scores) - 1} steps, best {scores[-1]}, {secs:.2f}s")
+    print("GA done", time.time() - t0)
 
 
 if __name__ == "__main__":

@@ -12,6 +12,7 @@
 """
 
 import ctypes as C
+import os
 
 import numpy as np
 import pytest
@@ -20,8 +21,10 @@ import bmmpy_b200 as bmm
 from bmmpy_b200 import _native as N
 from bmmpy_b200.matrix import BitMatrix
 from oracle import oracle as O
+from tests.golden.fixtures import GA_CASES
 
 pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
 
 def _instance(rows, cols, p, seed, scrambles):
@@ -168,6 +171,25 @@ def test_single_island_trajectory_matches_oracle(case):
     st = ga.stats()
     assert st.generations == len(want_scores) - 1 == ga.generation()
     assert st.evaluations == kw["population_size"] * (st.generations + 1)
+
+
+@pytest.mark.parametrize("case", range(len(GA_CASES)))
+def test_single_island_trajectory_matches_reference_golden(case):
+    """Against trajectories the reference GeneticAlgorithm itself produced,
+    including one on the full 256 x 8192 planted instance."""
+    wl = np.load(os.path.join(GOLDEN, "workloads.npz"))
+    rows, cols, p, iseed, scr, kw, steps, gseed = GA_CASES[case]
+    _, m, _ = _instance(rows, cols, p, iseed, scr)
+    ga = bmm.GeneticAlgorithm(seed=gseed, **kw)
+    ga.initialize(m.row_window(list(range(rows))))
+    got = [ga.best_score()]
+    while not ga.done() and len(got) <= steps:
+        ga.step()
+        got.append(ga.best_score())
+    assert got == wl[f"ga{case}_scores"].tolist()
+    best = ga.best_individual()
+    assert [c.mask for c in best] == wl[f"ga{case}_masks"].tolist()
+    assert [c.weight for c in best] == wl[f"ga{case}_weights"].tolist()
 
 
 def _ga_matrix():

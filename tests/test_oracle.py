@@ -13,10 +13,11 @@ import random
 import numpy as np
 import pytest
 
-from oracle.oracle import port, ref
+from oracle.oracle import ga_config, port, ref
 from tests.golden.fixtures import (
     C1,
     C2,
+    GA_CASES,
     batch_instance,
     checksum_pairs,
     cuda_equivalence_matrix,
@@ -144,6 +145,59 @@ def test_ga_kernels_small():
     P.local_improvement(m, 150, win, masks, weights)
     for i in range(n):
         assert weights[i] == P.eval_cand_weight(m, 150, win, masks[i])
+
+
+@pytest.mark.parametrize("case", range(len(GA_CASES)))
+def test_ga_port_matches_reference_golden(wl, case):
+    """The C GeneticAlgorithm restatement reproduces the reference's
+    trajectories (best score after every step) and best individuals."""
+    rows, cols, p, iseed, scr, kw, steps, gseed = GA_CASES[case]
+    m, _ = port().gen_instance(rows, cols, p, iseed, scr)
+    scores, bm, bw = port().ga_run(m, cols, list(range(rows)), ga_config(**kw), gseed, steps)
+    assert scores == wl[f"ga{case}_scores"].tolist()
+    assert np.array_equal(bm, wl[f"ga{case}_masks"])
+    assert np.array_equal(bw, wl[f"ga{case}_weights"])
+
+
+def test_ga_crossover_port_pads_with_unit_weight_one():
+    """crossover (operators.cpp:58-98): pool sorted by (weight, mask
+    popcount), stable; dependent candidates skipped; unit padding weighs 1."""
+    pm = np.array([[[0b011], [0b011], [0b000]], [[0b010], [0b110], [0b011]]], np.uint64)
+    pw = np.array([[5, 2, 0], [2, 9, 2]], np.uint32)
+    cm, cw = port().crossover(pm, pw)
+    # pool order: (0,w0 pc0) idx2, (2,pc1) idx3, (2,pc2) idx1, (2,pc2) idx5, (5) idx0, (9) idx4
+    # zero mask rejected; 0b010 -> pivot 1; 0b011 -> reduced 0b001 -> pivot 0; 0b011 (idx5)
+    # dependent; 0b011 (idx0) dependent; 0b110 -> reduced 0b100 -> pivot 2: full rank
+    assert cm[:, 0].tolist() == [0b010, 0b011, 0b110]
+    assert cw.tolist() == [2, 2, 9]
+    pm2 = np.array([[[0b001], [0b001], [0b000]]], np.uint64)
+    cm2, cw2 = port().crossover(pm2, np.array([[4, 3, 1]], np.uint32))
+    assert cm2[:, 0].tolist() == [0b001, 0b010, 0b100]
+    assert cw2.tolist() == [3, 1, 1]
+
+
+@pytest.mark.skipif(ref() is None, reason="reference library not built (make -C oracle ref)")
+def test_ga_port_matches_reference_random():
+    P, R = port(), ref()
+    rng = random.Random(11)
+    for trial in range(12):
+        rows = rng.randint(1, 40)
+        cols = rng.choice([1, 63, 64, 130, 300])
+        m, _ = P.gen_instance(rows, cols, rng.choice([0.05, 0.3]), rng.randint(0, 99),
+                              rng.randint(0, 3 * rows))
+        kw = dict(population_size=rng.randint(1, 20), elite_count=rng.randint(0, 4),
+                  tournament_size=rng.randint(0, 4), num_parents=rng.randint(1, 3),
+                  num_offspring=rng.randint(1, 3), mutation_rate=rng.choice([0.1, 0.3, 1.2]),
+                  enable_catastrophe=rng.random() < 0.3, catastrophe_threshold=rng.randint(0, 5),
+                  max_generations=rng.randint(0, 25))
+        if rng.random() < 0.3:
+            kw["max_stale_generations"] = rng.randint(1, 6)
+        win = rng.sample(range(rows), rng.randint(1, rows))
+        seed = rng.randint(0, 2**64 - 1)
+        a = P.ga_run(m, cols, win, ga_config(**kw), seed, 25)
+        b = R.ga_run(m, cols, win, ga_config(**kw), seed, 25)
+        assert a[0] == b[0]
+        assert np.array_equal(a[1], b[1]) and np.array_equal(a[2], b[2])
 
 
 @pytest.mark.skipif(ref() is None, reason="reference library not built (make -C oracle ref)")
