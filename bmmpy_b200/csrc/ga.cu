@@ -122,6 +122,10 @@ __device__ __forceinline__ uint4 vxor(uint4 a, uint4 b) {
     return make_uint4(a.x ^ b.x, a.y ^ b.y, a.z ^ b.z, a.w ^ b.w);
 }
 __device__ __forceinline__ uint2 vxor(uint2 a, uint2 b) { return make_uint2(a.x ^ b.x, a.y ^ b.y); }
+__device__ __forceinline__ uint4 vand(uint4 a, uint4 b) {
+    return make_uint4(a.x & b.x, a.y & b.y, a.z & b.z, a.w & b.w);
+}
+__device__ __forceinline__ uint2 vand(uint2 a, uint2 b) { return make_uint2(a.x & b.x, a.y & b.y); }
 __device__ __forceinline__ uint32_t vpopc(uint4 a) {
     return __popc(a.x) + __popc(a.y) + __popc(a.z) + __popc(a.w);
 }
@@ -246,8 +250,8 @@ __device__ void apply_pairs(uint64_t* T, uint64_t* M, uint8_t* touched, int N, u
 
 // Crossover (operators.cpp:58-98) of np parents of N candidates: the np*N
 // candidates stable-sorted by (weight, mask popcount) and inserted greedily
-// into a GF(2) basis with pivots at the highest set bit (PivotBasis,
-// xor_basis.hpp:117-155) until N are independent, then unit vectors pad the
+// into a GF(2) basis (PivotBasis, xor_basis.hpp:117-155: a candidate is kept
+// when independent of those kept before) until N are independent, then unit vectors pad the
 // basis with weight 1 (as the reference does; a full-rank parent makes the
 // padding unreachable).  Child candidate n: source row srcp[n] (parent
 // candidate row, or window row u for unit u), mask M[n], weight keepw[n].
@@ -300,53 +304,74 @@ __device__ void crossover(const uint64_t* const* pm, const uint32_t* const* pw,
             }
             __syncthreads();
         }
-    if (tid == 0) {
+    // Greedy insertion, warp 0.  The basis is kept fully reduced (each pivot
+    // row is zero in every other pivot column), so a candidate reduces in one
+    // step -- XOR of the pivot rows at its set pivot bits -- and lane l owns
+    // pivot rows l, l+32, ...  Independence does not depend on the basis
+    // representation, so the accepted candidates are PivotBasis's.
+    if (tid < 32) {
+        const int lane = tid;
         int nchild = 0;
         for (int q = 0; q < pool + N && nchild < N; ++q) {
             uint64_t v[4];
-            int id, unit = -1;
+            int id = -1, unit = -1;
             if (q < pool) {
                 id = (int)(sm.key[q] & 1023u);
 #pragma unroll
                 for (int w = 0; w < 4; ++w)
                     v[w] = sm.pmask[id * 4 + w];
             } else {
-                id = -1;
                 unit = q - pool;
                 v[0] = v[1] = v[2] = v[3] = 0;
                 v[unit >> 6] = 1ull << (unit & 63);
             }
-            for (;;) {
-                const int hb = highest_bit4(v);
-                if (hb < 0)
-                    break;
-                if (!sm.used[hb]) {
-                    sm.used[hb] = 1;
+            uint64_t r[4] = {0, 0, 0, 0};
+            for (int p = lane; p < N; p += 32)
+                if (sm.used[p] && ((v[p >> 6] >> (p & 63)) & 1ull)) {
 #pragma unroll
                     for (int w = 0; w < 4; ++w)
-                        sm.basis[hb * 4 + w] = v[w];
-                    // the child keeps the original candidate, not the reduced vector
-                    if (id >= 0) {
-                        const int p = id / N, n = id % N;
-                        srcp[nchild] = pr[p] + (size_t)n * W;
-#pragma unroll
-                        for (int w = 0; w < 4; ++w)
-                            M[nchild * 4 + w] = sm.pmask[id * 4 + w];
-                        keepw[nchild] = pw[p][n];
-                    } else {
-                        srcp[nchild] = base + (size_t)unit * W;
-#pragma unroll
-                        for (int w = 0; w < 4; ++w)
-                            M[nchild * 4 + w] = (unit >> 6) == w ? 1ull << (unit & 63) : 0ull;
-                        keepw[nchild] = 1;
-                    }
-                    ++nchild;
-                    break;
+                        r[w] ^= sm.basis[p * 4 + w];
                 }
 #pragma unroll
-                for (int w = 0; w < 4; ++w)
-                    v[w] ^= sm.basis[hb * 4 + w];
+            for (int w = 0; w < 4; ++w) {
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1)
+                    r[w] ^= __shfl_xor_sync(kFull, r[w], o);
+                r[w] ^= v[w];
             }
+            const int hb = highest_bit4(r);
+            if (hb < 0)
+                continue;  // dependent
+            for (int p = lane; p < N; p += 32)
+                if (sm.used[p] && ((sm.basis[p * 4 + (hb >> 6)] >> (hb & 63)) & 1ull)) {
+#pragma unroll
+                    for (int w = 0; w < 4; ++w)
+                        sm.basis[p * 4 + w] ^= r[w];
+                }
+            __syncwarp();
+            if (lane == 0) {
+                sm.used[hb] = 1;
+#pragma unroll
+                for (int w = 0; w < 4; ++w)
+                    sm.basis[hb * 4 + w] = r[w];
+                // the child keeps the original candidate, not the reduced vector
+                if (id >= 0) {
+                    const int p = id / N, n = id % N;
+                    srcp[nchild] = pr[p] + (size_t)n * W;
+#pragma unroll
+                    for (int w = 0; w < 4; ++w)
+                        M[nchild * 4 + w] = sm.pmask[id * 4 + w];
+                    keepw[nchild] = pw[p][n];
+                } else {
+                    srcp[nchild] = base + (size_t)unit * W;
+#pragma unroll
+                    for (int w = 0; w < 4; ++w)
+                        M[nchild * 4 + w] = (unit >> 6) == w ? 1ull << (unit & 63) : 0ull;
+                    keepw[nchild] = 1;
+                }
+            }
+            __syncwarp();
+            ++nchild;
         }
     }
     __syncthreads();
@@ -1038,23 +1063,222 @@ __host__ __device__ inline size_t local_smem_bytes() {
     return (size_t)2 * kLiTile * (kLiChunk + 1) * 8;
 }
 
+// Local improvement with the overlap matrix in shared memory (u16: rows of at
+// most 1023 words, so every overlap fits).  Same moves as local_improve.  The
+// warps scan consecutive rows i at once (nothing changes before a move, so
+// every scan is the one the sequential pass would make) and the smallest
+// improving i wins; the whole CTA then applies the move and recomputes row and
+// column i of G (four rows per warp, eight 16-byte or 8-byte loads in flight
+// per lane; the moved row itself from shared memory).  s_move: 4 ints then 32
+// u64 of scratch.
+constexpr int kLi16Chunk = 64;
+constexpr int kLi16MaxW = 1023;  // 64 * 1023 < 65536: overlaps fit in u16
+
+// G (u16) rounded up to 16 bytes so that the 64-bit tiles after it are aligned.
+__host__ __device__ inline size_t local16_g_bytes(int N) {
+    return ((size_t)N * N * 2 + 15) & ~(size_t)15;
+}
+
+__host__ __device__ inline size_t local16_smem_bytes(int N) {
+    return local16_g_bytes(N) + (size_t)2 * kLiTile * (kLi16Chunk + 1) * 8;
+}
+
+template <typename V>
+__device__ void overlap_row(const uint64_t* R, const uint64_t* rnew, int N, int W, int i,
+                            uint16_t* G) {
+    constexpr int kPer = (int)(sizeof(V) / 8);
+    const int W2 = W / kPer;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const V* ri = reinterpret_cast<const V*>(rnew);  // row i after the move (shared)
+    for (int k0 = warp * 4; k0 < N; k0 += nw * 4) {
+        uint32_t pc[4] = {0, 0, 0, 0};
+        for (int e0 = 0; e0 < W2; e0 += 64) {
+            V a[2], b[4][2];
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int e = e0 + lane + 32 * u;
+                a[u] = e < W2 ? ri[e] : vzero<V>();
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int k = k0 + r;
+                const V* rk = k == i ? ri
+                                     : reinterpret_cast<const V*>(R + (size_t)(k < N ? k : 0) * W);
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int e = e0 + lane + 32 * u;
+                    b[r][u] = (k < N && e < W2) ? rk[e] : vzero<V>();
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int u = 0; u < 2; ++u)
+                    pc[r] += vpopc(vand(a[u], b[r][u]));
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            uint32_t t = pc[r];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
+                t += __shfl_xor_sync(kFull, t, o);
+            const int k = k0 + r;
+            if (lane == 0 && k < N) {
+                G[i * N + k] = (uint16_t)t;
+                G[k * N + i] = (uint16_t)t;
+            }
+        }
+    }
+}
+
+__device__ void local_improve16(uint64_t* R, uint64_t* M, uint32_t* Wt, int N, int W,
+                                unsigned char* smem, uint32_t* w, int* s_move) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    uint16_t* G = reinterpret_cast<uint16_t*>(smem);
+    uint64_t* A = reinterpret_cast<uint64_t*>(smem + local16_g_bytes(N));
+    uint64_t* B = A + kLiTile * (kLi16Chunk + 1);
+    constexpr int WS = kLi16Chunk + 1;
+    const int ntile = (N + kLiTile - 1) / kLiTile;
+    const int per = (kLiTile * kLiTile) / blockDim.x;
+    const int ti_div = kLiTile / per;
+    for (int ti = 0; ti < ntile; ++ti)
+        for (int tj = ti; tj < ntile; ++tj) {
+            uint32_t acc[4] = {0, 0, 0, 0};
+            for (int w0 = 0; w0 < W; w0 += kLi16Chunk) {
+                const int wc = min(kLi16Chunk, W - w0);
+                __syncthreads();
+                for (int e = tid; e < kLiTile * wc; e += blockDim.x) {
+                    const int r = e / wc, q = e % wc;
+                    const int ra = ti * kLiTile + r, rb = tj * kLiTile + r;
+                    A[r * WS + q] = ra < N ? R[(size_t)ra * W + w0 + q] : 0ull;
+                    B[r * WS + q] = rb < N ? R[(size_t)rb * W + w0 + q] : 0ull;
+                }
+                __syncthreads();
+                const int i = tid / ti_div, j0 = (tid % ti_div) * per;
+                const uint64_t* a = A + i * WS;
+                for (int q = 0; q < wc; ++q) {
+                    const uint64_t av = a[q];
+                    for (int u = 0; u < per; ++u)
+                        acc[u] += __popcll(av & B[(j0 + u) * WS + q]);
+                }
+            }
+            const int i = tid / ti_div, j0 = (tid % ti_div) * per;
+            const int gi = ti * kLiTile + i;
+            for (int u = 0; u < per; ++u) {
+                const int gj = tj * kLiTile + j0 + u;
+                if (gi < N && gj < N) {
+                    G[gi * N + gj] = (uint16_t)acc[u];
+                    G[gj * N + gi] = (uint16_t)acc[u];
+                }
+            }
+        }
+    __syncthreads();
+    for (int i = tid; i < N; i += blockDim.x)
+        w[i] = G[i * N + i];  // re-materialised weights
+    __syncthreads();
+    // After the overlap matrix is built the tiles are free: the moved row is
+    // staged there (W words; rows wider than the tile area use global memory).
+    uint64_t* rnew = A;
+    const bool rnew_shared = (size_t)W * 8 <= (size_t)2 * kLiTile * (kLi16Chunk + 1) * 8;
+    const int nw = blockDim.x >> 5;
+    unsigned long long* s_found = reinterpret_cast<unsigned long long*>(s_move + 4);
+    for (int iter = 0; iter < 10; ++iter) {
+        int improved = 0;
+        int start = 0;
+        for (;;) {
+            // warps scan rows start + warp, start + nw + warp, ... in rounds;
+            // the first round with an improving row decides (its smallest i)
+            int fi = -1;
+            unsigned long long fk = 0;
+            for (int base = start; base < N; base += nw) {
+                const int i = base + warp;
+                unsigned long long best = ~0ull;
+                const uint32_t wi = i < N ? w[i] : 0u;
+                if (wi != 0) {
+                    for (int j = lane; j < N; j += 32) {
+                        const uint32_t wj = w[j];
+                        if (j == i || (unsigned long long)wj >= 2ull * wi)
+                            continue;
+                        const uint32_t cw = wi + wj - 2u * (uint32_t)G[i * N + j];
+                        if (cw < wi) {
+                            const unsigned long long k = ((unsigned long long)cw << 32) | (uint32_t)j;
+                            best = k < best ? k : best;
+                        }
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) {
+                        const unsigned long long ot = __shfl_xor_sync(kFull, best, o);
+                        best = ot < best ? ot : best;
+                    }
+                }
+                if (lane == 0)
+                    s_found[warp] = best;
+                __syncthreads();
+                for (int q = 0; q < nw; ++q)
+                    if (s_found[q] != ~0ull) {
+                        fi = base + q;
+                        fk = s_found[q];
+                        break;
+                    }
+                __syncthreads();
+                if (fi >= 0)
+                    break;
+            }
+            if (fi < 0)
+                break;
+            const int i = fi, j = (int)(fk & 0xffffffffu);
+            const uint32_t cw = (uint32_t)(fk >> 32);
+            uint64_t* rn = rnew_shared ? rnew : R + (size_t)i * W;
+            for (int q = tid; q < W; q += blockDim.x) {
+                const uint64_t v = R[(size_t)i * W + q] ^ R[(size_t)j * W + q];
+                rn[q] = v;
+                if (rnew_shared)
+                    R[(size_t)i * W + q] = v;
+            }
+            if (tid < 4)
+                M[i * 4 + tid] ^= M[j * 4 + tid];
+            __syncthreads();
+            if ((W & 1) == 0)
+                overlap_row<uint4>(R, rn, N, W, i, G);
+            else
+                overlap_row<uint2>(R, rn, N, W, i, G);
+            if (tid == 0)
+                w[i] = cw;
+            __syncthreads();
+            improved = 1;
+            start = i + 1;
+        }
+        if (!improved)
+            break;
+    }
+    for (int i = tid; i < N; i += blockDim.x)
+        Wt[i] = w[i];
+    __syncthreads();
+}
+
 // Children (slot kind kChild) of stepped islands, next population.
+template <bool kSmemG>
 __global__ void __launch_bounds__(kLocalThreads) local_kernel(State st) {
-    extern __shared__ __align__(16) uint64_t tiles[];
+    extern __shared__ __align__(16) unsigned char lsmem[];
     __shared__ uint32_t w[kMaxN];
     __shared__ unsigned long long s_best[64];
-    __shared__ int s_flag;
+    __shared__ __align__(8) int s_flag[4 + 2 * 32];
     const Config& c = st.c;
     const int N = c.N, W = c.W, P = c.P;
     uint32_t* G = st.Gs + (size_t)blockIdx.x * N * N;
+    uint64_t* tiles = reinterpret_cast<uint64_t*>(lsmem);
     for (uint32_t cs = blockIdx.x; cs < (uint32_t)(st.I * P); cs += gridDim.x) {
         const IslandStat& is = st.stat[cs / P];
         if (!is.stepped || st.sched[cs].kind != kChild)
             continue;
         const Pop p = st.pop[is.cur ^ 1];
-        local_improve(p.rows + (size_t)cs * N * W, p.masks + (size_t)cs * N * 4,
-                      p.wts + (size_t)cs * N, N, W, G, tiles, tiles + kLiTile * (kLiChunk + 1), w,
-                      s_best, &s_flag);
+        if (kSmemG)
+            local_improve16(p.rows + (size_t)cs * N * W, p.masks + (size_t)cs * N * 4,
+                            p.wts + (size_t)cs * N, N, W, lsmem, w, s_flag);
+        else
+            local_improve(p.rows + (size_t)cs * N * W, p.masks + (size_t)cs * N * 4,
+                          p.wts + (size_t)cs * N, N, W, G, tiles,
+                          tiles + kLiTile * (kLiChunk + 1), w, s_best, &s_flag[0]);
     }
 }
 
@@ -1137,9 +1361,12 @@ __global__ void __launch_bounds__(kLocalThreads) op_kernel(int op, const uint64_
         uint64_t* A = reinterpret_cast<uint64_t*>(smem);
         __shared__ uint32_t w[kMaxN];
         __shared__ unsigned long long s_best[64];
-        __shared__ int s_flag;
-        local_improve(rows, masks, wts, N, W, G, A, A + kLiTile * (kLiChunk + 1), w, s_best,
-                      &s_flag);
+        __shared__ __align__(8) int s_flag[4 + 2 * 32];
+        if (W <= kLi16MaxW)
+            local_improve16(rows, masks, wts, N, W, smem, w, s_flag);
+        else
+            local_improve(rows, masks, wts, N, W, G, A, A + kLiTile * (kLiChunk + 1), w, s_best,
+                          &s_flag[0]);
     } else if (op == 2) {
         const uint64_t* pm[4];
         const uint32_t* pw[4];
@@ -1306,8 +1533,12 @@ int ga_generation(bmm_ga* g) {
     cudaStream_t s = g->stream;
     schedule_kernel<<<(I + 3) / 4, 128, 0, s>>>(st);
     build_kernel<<<g->build_grid, kBuildThreads, g->build_smem, s>>>(st, 0);
-    if (g->gen % 3 == 0)  // k_local_improvement_period
-        local_kernel<<<g->local_grid, kLocalThreads, local_smem_bytes(), s>>>(st);
+    if (g->gen % 3 == 0) {  // k_local_improvement_period
+        if (c.W <= kLi16MaxW)
+            local_kernel<true><<<g->local_grid, kLocalThreads, local16_smem_bytes(c.N), s>>>(st);
+        else
+            local_kernel<false><<<g->local_grid, kLocalThreads, local_smem_bytes(), s>>>(st);
+    }
     const int fit_blocks = (int)(((size_t)I * P * 32 + 255) / 256);
     fitness_kernel<<<fit_blocks, 256, 0, s>>>(st, 1);
     bool mig = false;  // some island exports after this generation
@@ -1375,7 +1606,8 @@ int op_alloc(void** p, size_t bytes) {
 }
 
 size_t op_smem(int N, int np) {
-    return std::max(build_smem_bytes(N, np > 0 ? np : 1), local_smem_bytes());
+    return std::max(std::max(build_smem_bytes(N, np > 0 ? np : 1), local_smem_bytes()),
+                    local16_smem_bytes(N));
 }
 
 }  // namespace
@@ -1466,7 +1698,7 @@ BMM_API int bmm_ga_create(const uint64_t* words, size_t stride, size_t cols, con
     g->rank_threads = pow2_at_least(P);
     g->build_smem = build_smem_bytes(N, c.parents);
     g->build_grid = ws->sm_count * 4;
-    g->local_grid = ws->sm_count * 2;
+    g->local_grid = W <= kLi16MaxW ? ws->sm_count : ws->sm_count * 2;
 
     const std::vector<uint64_t> base = compact_window(words, stride, cols, win, n);
     std::vector<uint64_t> jm((size_t)(N + 1) * 64), jr(64);
@@ -1536,7 +1768,7 @@ BMM_API int bmm_ga_create(const uint64_t* words, size_t stride, size_t cols, con
     S.best_masks = (uint64_t*)A(islands * N * 32);
     S.best_rows = (uint64_t*)A(islands * N * W * 8);
     S.best_wts = (uint32_t*)A(islands * N * 4);
-    S.Gs = (uint32_t*)A((size_t)g->local_grid * N * N * 4);
+    S.Gs = (uint32_t*)A(W <= kLi16MaxW ? 16 : (size_t)g->local_grid * N * N * 4);
     if (rc != BMM_OK) {
         ga_free(g);
         return rc;
@@ -1566,8 +1798,11 @@ BMM_API int bmm_ga_create(const uint64_t* words, size_t stride, size_t cols, con
         e = cudaFuncSetAttribute(build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)g->build_smem);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(local_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(local_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)local_smem_bytes());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(local_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)local16_smem_bytes(N));
     if (e != cudaSuccess) {
         ga_free(g);
         return fail(BMM_ECUDA, "ga: setup failed: %s", cudaGetErrorString(e));
