@@ -39,6 +39,7 @@ _sz = C.c_size_t
 _szp = C.POINTER(C.c_size_t)
 _vp = C.c_void_p
 _candp = C.POINTER(Candidate_t)
+_f32p = C.POINTER(C.c_float)
 
 
 class Instance_t(C.Structure):
@@ -115,9 +116,18 @@ SIGNATURES = {
     "bmm_ga_mutate": [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, C.c_double, _u64p],
     "bmm_ga_local_improve": [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p],
     "bmm_ga_crossover": [_sz, _sz, _u64p, _u32p, _u64p, _u32p],
+    "bmm_mlp_create": [C.c_uint64, C.c_float, C.POINTER(_vp)],
+    "bmm_mlp_destroy": [_vp],
+    "bmm_mlp_param_count": [],
+    "bmm_mlp_get_params": [_vp, _f32p],
+    "bmm_mlp_set_params": [_vp, _f32p],
+    "bmm_mlp_forward": [_vp, _f32p, _sz, _f32p],
+    "bmm_mlp_grads": [_vp, _f32p, _f32p, _sz, _f32p, _f32p],
+    "bmm_mlp_train": [_vp, _f32p, _f32p, _sz, C.c_int, _f32p],
+    "bmm_mlp_gemm": [_f32p, _f32p, C.c_int, C.c_int, C.c_int, _f32p],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
-             "bmm_gen_instance": C.c_uint64}
+             "bmm_gen_instance": C.c_uint64, "bmm_mlp_param_count": C.c_size_t}
 
 _lib = None
 
@@ -171,6 +181,10 @@ def u64p(a):
 
 def u32p(a):
     return ptr(a, _u32p)
+
+
+def f32p(a):
+    return ptr(a, _f32p)
 
 
 def szp(a):

@@ -1,0 +1,672 @@
+// Proposal network for the genetic algorithm: a 512 -> 256 -> 256 -> 256 MLP
+// (ReLU) whose three GEMMs run on the 5th-generation tensor cores (tcgen05,
+// BF16 operands, FP32 accumulators in TMEM), with hand-written backward and
+// Adam kernels.  No reference counterpart: the reference GA draws its
+// mutation partners uniformly (operators.cpp:100-129).
+//
+// Inputs per query (a target row i of an individual): 256 per-row weight
+// features and the ±1 bits of row i's 256-column sketch; outputs: one logit
+// per candidate row j (how likely j belongs to an improving XOR subset for i).
+//
+// GEMM kernel.  C[M x N] = A[M x K] . B[N x K]^T for any element strides of A
+// and B (transposes are folded into the staging loads), FP32 or BF16 sources
+// rounded to BF16 while they are written to shared memory in the canonical
+// K-major layout; one CTA per 128 x 256 output tile, K in chunks of 64 (four
+// K=16 MMAs per chunk), TMEM accumulator of 256 columns; the epilogue reads
+// TMEM (tcgen05.ld 32x32b) and applies scale, bias, the ReLU-backward mask and
+// ReLU, writing FP32 (pre-activation) and/or BF16 (activation) outputs.
+#include "common.cuh"
+#include "umma.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace bmm {
+namespace mlp {
+
+constexpr int kIn = 512, kHid = 256, kOut = 256;
+constexpr size_t kW1 = 0, kB1 = kW1 + (size_t)kHid * kIn, kW2 = kB1 + kHid,
+                 kB2 = kW2 + (size_t)kHid * kHid, kW3 = kB2 + kHid,
+                 kB3 = kW3 + (size_t)kOut * kHid, kParams = kB3 + kOut;
+
+constexpr int kBM = 128, kBN = 256, kBK = 64;
+constexpr int kGemmThreads = 128;
+constexpr uint32_t kWaitLimit = 1u << 22;
+// 48 KB of operand tiles; asking for more keeps at most two CTAs (2 x 256
+// TMEM columns) resident per SM.
+constexpr size_t kGemmSmem = 100 * 1024;
+
+struct GemmArgs {
+    const void* A;
+    int a_bf16;
+    long long lda_m, lda_k;
+    const void* B;
+    int b_bf16;
+    long long ldb_n, ldb_k;
+    int M, N, K;
+    float scale;
+    const float* bias;       // [N] or null
+    const float* relu_mask;  // [M][ldm]: output *= (mask > 0), or null
+    long long ldm;
+    int relu;                // the BF16 output is max(value, 0)
+    float* out_f;            // value before ReLU, [M][ldo_f], or null
+    long long ldo_f;
+    __nv_bfloat16* out_b;    // [M][ldo_b], or null
+    long long ldo_b;
+    int* err;
+};
+
+__device__ __forceinline__ float load_elem(const void* p, int bf16, long long idx) {
+    return bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[idx])
+                : reinterpret_cast<const float*>(p)[idx];
+}
+
+// rows x kBK tile, element (r, k) = src[(row0 + r) * ld_r + (k0 + k) * ld_k],
+// zero outside [0, nrows) x [0, K).
+__device__ void stage(unsigned char* dst, int rows, const void* src, int bf16, long long ld_r,
+                      long long ld_k, int row0, int nrows, int k0, int K) {
+    const int total = rows * kBK;
+    const bool kfast = ld_k == 1 || ld_r != 1;  // walk the contiguous index fastest
+    for (int e = threadIdx.x; e < total; e += blockDim.x) {
+        int r, k;
+        if (kfast) {
+            r = e / kBK;
+            k = e % kBK;
+        } else {
+            k = e / rows;
+            r = e % rows;
+        }
+        const int gr = row0 + r, gk = k0 + k;
+        float v = 0.f;
+        if (gr < nrows && gk < K)
+            v = load_elem(src, bf16, (long long)gr * ld_r + (long long)gk * ld_k);
+        *reinterpret_cast<__nv_bfloat16*>(dst + umma::kmajor_offset(r, k, kBK)) =
+            __float2bfloat16_rn(v);
+    }
+}
+
+__global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char* sA = smem;
+    unsigned char* sB = smem + kBM * kBK * 2;
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    if (warp == 0)
+        umma::tmem_alloc(&tmem_slot, 256);
+    if (tid == 0) {
+        umma::mbar_init(umma::smem_u32(&mbar), 1);
+        s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    const uint32_t idesc = umma::idesc_bf16(kBM, kBN);
+    const int nk = (g.K + kBK - 1) / kBK;
+    int kc = 0;
+    for (; kc < nk; ++kc) {
+        stage(sA, kBM, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M, kc * kBK, g.K);
+        stage(sB, kBN, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N, kc * kBK, g.K);
+        umma::fence_async_smem();
+        __syncthreads();
+        if (tid == 0) {
+            umma::fence_after_sync();
+            const uint32_t a0 = umma::smem_u32(sA), b0 = umma::smem_u32(sB);
+#pragma unroll
+            for (int s = 0; s < kBK / 16; ++s) {
+                const uint64_t da = umma::smem_desc(a0 + s * 256, 128, (kBK / 8) * 128);
+                const uint64_t db = umma::smem_desc(b0 + s * 256, 128, (kBK / 8) * 128);
+                umma::mma_bf16(tmem, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
+            }
+            umma::commit(umma::smem_u32(&mbar));
+        }
+        if (!umma::mbar_wait(umma::smem_u32(&mbar), kc & 1, kWaitLimit))
+            s_fail = 1;
+        __syncthreads();
+        if (s_fail)
+            break;
+    }
+    umma::fence_after_sync();
+    if (!s_fail) {
+        const int m = m0 + warp * 32 + lane;
+        for (int c = 0; c < kBN / 32; ++c) {
+            float v[32];
+            umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), v);
+            if (m >= g.M)
+                continue;
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int n = n0 + c * 32 + i;
+                if (n >= g.N)
+                    continue;
+                float val = v[i] * g.scale;
+                if (g.bias)
+                    val += g.bias[n];
+                if (g.relu_mask && !(g.relu_mask[(long long)m * g.ldm + n] > 0.f))
+                    val = 0.f;
+                if (g.out_f)
+                    g.out_f[(long long)m * g.ldo_f + n] = val;
+                if (g.out_b)
+                    g.out_b[(long long)m * g.ldo_b + n] =
+                        __float2bfloat16_rn(g.relu ? fmaxf(val, 0.f) : val);
+            }
+        }
+    } else {
+        if (tid == 0)
+            atomicExch(g.err, 1);
+        // let the MMAs in flight finish (bounded) before the TMEM is released
+        umma::mbar_wait(umma::smem_u32(&mbar), kc & 1, kWaitLimit);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, 256);
+    }
+}
+
+// Softmax cross-entropy against target distributions: warp per row.
+// dlogits = (softmax - target) / rows; *loss += -sum(target * log softmax) / rows.
+__global__ void xent_kernel(const float* __restrict__ logits, const float* __restrict__ target,
+                            float* __restrict__ dlogits, float* loss, int rows) {
+    const int lane = threadIdx.x & 31;
+    const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= rows)
+        return;
+    const float* z = logits + (size_t)r * kOut;
+    const float* t = target + (size_t)r * kOut;
+    float v[kOut / 32];
+    float mx = -INFINITY;
+#pragma unroll
+    for (int q = 0; q < kOut / 32; ++q) {
+        v[q] = z[lane + 32 * q];
+        mx = fmaxf(mx, v[q]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(kFull, mx, o));
+    float se = 0.f;
+#pragma unroll
+    for (int q = 0; q < kOut / 32; ++q)
+        se += expf(v[q] - mx);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        se += __shfl_xor_sync(kFull, se, o);
+    const float lse = mx + logf(se);
+    float l = 0.f;
+    const float inv = 1.f / (float)rows;
+#pragma unroll
+    for (int q = 0; q < kOut / 32; ++q) {
+        const int j = lane + 32 * q;
+        const float p = expf(v[q] - lse);
+        const float tj = t[j];
+        dlogits[(size_t)r * kOut + j] = (p - tj) * inv;
+        if (tj != 0.f)
+            l -= tj * (v[q] - lse);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+        l += __shfl_xor_sync(kFull, l, o);
+    if (lane == 0 && loss)
+        atomicAdd(loss, l * inv);
+}
+
+// Column sums of a [rows][256] matrix (bias gradients).
+__global__ void colsum_kernel(const float* __restrict__ d, int rows, float* __restrict__ out) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= kOut)
+        return;
+    float s = 0.f;
+    for (int r = 0; r < rows; ++r)
+        s += d[(size_t)r * kOut + n];
+    out[n] = s;
+}
+
+// Adam (Kingma & Ba) with bias correction on the FP32 master parameters.
+__global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                            const float* __restrict__ grad, size_t n, float lr, float b1, float b2,
+                            float eps, float c1, float c2) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    const float g = grad[i];
+    const float mi = b1 * m[i] + (1.f - b1) * g;
+    const float vi = b2 * v[i] + (1.f - b2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+}  // namespace mlp
+}  // namespace bmm
+
+using namespace bmm;
+using namespace bmm::mlp;
+
+// Network state: parameters, Adam moments, gradients and activation scratch
+// for up to `cap` rows, all device-resident.
+struct bmm_mlp {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    float* w = nullptr;  // kParams
+    float* m = nullptr;
+    float* v = nullptr;
+    float* g = nullptr;
+    long long step = 0;
+    float lr = 1e-3f, b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    size_t cap = 0;
+    float* z1 = nullptr;  // [cap][256] pre-activations
+    float* z2 = nullptr;
+    float* z3 = nullptr;  // logits
+    __nv_bfloat16* h1 = nullptr;
+    __nv_bfloat16* h2 = nullptr;
+    float* dz3 = nullptr;
+    float* dz2 = nullptr;
+    float* dz1 = nullptr;
+    float* x = nullptr;  // [cap][512] staging for host inputs
+    float* t = nullptr;  // [cap][256] targets
+    float* loss = nullptr;
+    int* err = nullptr;
+};
+
+namespace {
+
+int gemm_launch(const GemmArgs& a, cudaStream_t s) {
+    static thread_local int attr_dev = -1;
+    int dev = -1;
+    cudaGetDevice(&dev);
+    if (attr_dev != dev) {
+        BMM_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kGemmSmem));
+        attr_dev = dev;
+    }
+    dim3 grid((a.M + kBM - 1) / kBM, (a.N + kBN - 1) / kBN);
+    gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(a);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(BMM_ECUDA, "mlp: gemm launch failed: %s", cudaGetErrorString(e));
+    return BMM_OK;
+}
+
+GemmArgs gemm_args(const void* A, int a_bf16, long long lda_m, long long lda_k, const void* B,
+                   int b_bf16, long long ldb_n, long long ldb_k, int M, int N, int K, int* err) {
+    GemmArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.A = A;
+    a.a_bf16 = a_bf16;
+    a.lda_m = lda_m;
+    a.lda_k = lda_k;
+    a.B = B;
+    a.b_bf16 = b_bf16;
+    a.ldb_n = ldb_n;
+    a.ldb_k = ldb_k;
+    a.M = M;
+    a.N = N;
+    a.K = K;
+    a.scale = 1.f;
+    a.err = err;
+    return a;
+}
+
+int check_err(bmm_mlp* h) {
+    int e = 0;
+    BMM_CUDA_TRY(cudaMemcpyAsync(&e, h->err, 4, cudaMemcpyDeviceToHost, h->stream));
+    BMM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (e)
+        return fail(BMM_ETIMEOUT, "mlp: a tensor-core wait timed out");
+    return BMM_OK;
+}
+
+int ensure_cap(bmm_mlp* h, size_t rows) {
+    if (rows <= h->cap)
+        return BMM_OK;
+    size_t cap = std::max<size_t>(rows, 256);
+    float** fs[] = {&h->z1, &h->z2, &h->z3, &h->dz3, &h->dz2, &h->dz1, &h->t};
+    for (float** p : fs) {
+        cudaFree(*p);
+        *p = nullptr;
+    }
+    cudaFree(h->h1);
+    cudaFree(h->h2);
+    cudaFree(h->x);
+    h->h1 = h->h2 = nullptr;
+    h->x = nullptr;
+    h->cap = 0;
+    cudaError_t e = cudaSuccess;
+    for (float** p : fs)
+        if (e == cudaSuccess)
+            e = cudaMalloc(p, cap * 256 * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&h->h1, cap * 256 * 2);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&h->h2, cap * 256 * 2);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&h->x, cap * kIn * 4);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(BMM_ENOMEM, "mlp: scratch allocation failed: %s", cudaGetErrorString(e));
+    }
+    h->cap = cap;
+    return BMM_OK;
+}
+
+}  // namespace
+
+namespace bmm {
+namespace mlp {
+
+// Forward pass of `rows` inputs X (FP32 or BF16, row stride kIn) into the
+// handle's scratch: z1/h1, z2/h2, logits z3 (or `logits` if given).
+int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) {
+    GemmArgs a = gemm_args(X, x_bf16, kIn, 1, h->w + kW1, 0, kIn, 1, rows, kHid, kIn, h->err);
+    a.bias = h->w + kB1;
+    a.relu = 1;
+    a.out_f = h->z1;
+    a.ldo_f = kHid;
+    a.out_b = h->h1;
+    a.ldo_b = kHid;
+    BMM_TRY(gemm_launch(a, h->stream));
+    a = gemm_args(h->h1, 1, kHid, 1, h->w + kW2, 0, kHid, 1, rows, kHid, kHid, h->err);
+    a.bias = h->w + kB2;
+    a.relu = 1;
+    a.out_f = h->z2;
+    a.ldo_f = kHid;
+    a.out_b = h->h2;
+    a.ldo_b = kHid;
+    BMM_TRY(gemm_launch(a, h->stream));
+    a = gemm_args(h->h2, 1, kHid, 1, h->w + kW3, 0, kHid, 1, rows, kOut, kHid, h->err);
+    a.bias = h->w + kB3;
+    a.out_f = logits ? logits : h->z3;
+    a.ldo_f = kOut;
+    return gemm_launch(a, h->stream);
+}
+
+// Gradients of the mean cross-entropy for the forward pass just run (rows,
+// targets T [rows][256]) into h->g; the loss is added to *h->loss.
+int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows) {
+    cudaStream_t s = h->stream;
+    xent_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(h->z3, T, h->dz3, h->loss, rows);
+    // dW3 = dZ3^T H2, db3
+    GemmArgs a = gemm_args(h->dz3, 0, 1, kOut, h->h2, 1, 1, kHid, kOut, kHid, rows, h->err);
+    a.out_f = h->g + kW3;
+    a.ldo_f = kHid;
+    BMM_TRY(gemm_launch(a, s));
+    colsum_kernel<<<1, 256, 0, s>>>(h->dz3, rows, h->g + kB3);
+    // dZ2 = (dZ3 W3) * (Z2 > 0)
+    a = gemm_args(h->dz3, 0, kOut, 1, h->w + kW3, 0, 1, kHid, rows, kHid, kOut, h->err);
+    a.relu_mask = h->z2;
+    a.ldm = kHid;
+    a.out_f = h->dz2;
+    a.ldo_f = kHid;
+    BMM_TRY(gemm_launch(a, s));
+    // dW2 = dZ2^T H1, db2
+    a = gemm_args(h->dz2, 0, 1, kHid, h->h1, 1, 1, kHid, kHid, kHid, rows, h->err);
+    a.out_f = h->g + kW2;
+    a.ldo_f = kHid;
+    BMM_TRY(gemm_launch(a, s));
+    colsum_kernel<<<1, 256, 0, s>>>(h->dz2, rows, h->g + kB2);
+    // dZ1 = (dZ2 W2) * (Z1 > 0)
+    a = gemm_args(h->dz2, 0, kHid, 1, h->w + kW2, 0, 1, kHid, rows, kHid, kHid, h->err);
+    a.relu_mask = h->z1;
+    a.ldm = kHid;
+    a.out_f = h->dz1;
+    a.ldo_f = kHid;
+    BMM_TRY(gemm_launch(a, s));
+    // dW1 = dZ1^T X (N = 512: two column tiles), db1
+    a = gemm_args(h->dz1, 0, 1, kHid, X, x_bf16, 1, kIn, kHid, kIn, rows, h->err);
+    a.out_f = h->g + kW1;
+    a.ldo_f = kIn;
+    BMM_TRY(gemm_launch(a, s));
+    colsum_kernel<<<1, 256, 0, s>>>(h->dz1, rows, h->g + kB1);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(BMM_ECUDA, "mlp: backward launch failed: %s", cudaGetErrorString(e));
+    return BMM_OK;
+}
+
+int adam_dev(bmm_mlp* h) {
+    h->step += 1;
+    const float c1 = 1.f - (float)std::pow((double)h->b1, (double)h->step);
+    const float c2 = 1.f - (float)std::pow((double)h->b2, (double)h->step);
+    adam_kernel<<<(unsigned)((kParams + 255) / 256), 256, 0, h->stream>>>(
+        h->w, h->m, h->v, h->g, kParams, h->lr, h->b1, h->b2, h->eps, c1, c2);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(BMM_ECUDA, "mlp: adam launch failed: %s", cudaGetErrorString(e));
+    return BMM_OK;
+}
+
+// One optimizer step on device inputs; loss (mean cross-entropy) to *loss_out.
+int train_step_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows) {
+    BMM_TRY(ensure_cap(h, (size_t)rows));
+    BMM_CUDA_TRY(cudaMemsetAsync(h->loss, 0, 4, h->stream));
+    BMM_TRY(forward_dev(h, X, x_bf16, rows, nullptr));
+    BMM_TRY(backward_dev(h, X, x_bf16, T, rows));
+    return adam_dev(h);
+}
+
+}  // namespace mlp
+}  // namespace bmm
+
+namespace {
+
+// Glorot-uniform weights from a xorshift64 stream, zero biases.
+void init_params(std::vector<float>& p, uint64_t seed) {
+    uint64_t s = seed ? seed : 0x9E3779B97F4A7C15ull;
+    auto unit = [&]() {
+        s ^= s << 13;
+        s ^= s >> 7;
+        s ^= s << 17;
+        return (double)(s >> 11) * (1.0 / 9007199254740992.0);
+    };
+    p.assign(kParams, 0.f);
+    auto fill = [&](size_t off, int out, int in) {
+        const double a = std::sqrt(6.0 / (double)(in + out));
+        for (size_t i = 0; i < (size_t)out * in; ++i)
+            p[off + i] = (float)((2.0 * unit() - 1.0) * a);
+    };
+    fill(kW1, kHid, kIn);
+    fill(kW2, kHid, kHid);
+    fill(kW3, kOut, kHid);
+}
+
+void mlp_free(bmm_mlp* h) {
+    if (!h)
+        return;
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    float* fs[] = {h->w, h->m, h->v, h->g, h->z1, h->z2, h->z3, h->dz3, h->dz2, h->dz1, h->x,
+                   h->t, h->loss};
+    for (float* p : fs)
+        cudaFree(p);
+    cudaFree(h->h1);
+    cudaFree(h->h2);
+    cudaFree(h->err);
+    if (h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+}  // namespace
+
+extern "C" {
+
+BMM_API int bmm_mlp_create(uint64_t seed, float learning_rate, bmm_mlp** out) {
+    clear_error();
+    if (!out)
+        return fail(BMM_EINVAL, "mlp: null output");
+    *out = nullptr;
+    if (!(learning_rate > 0.f))
+        return fail(BMM_EINVAL, "mlp: learning rate must be positive");
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    if (ws->sm_count <= 0)
+        return fail(BMM_ENODEV, "mlp: no CUDA device");
+    bmm_mlp* h = new bmm_mlp();
+    h->device = ws->device;
+    h->lr = learning_rate;
+    std::vector<float> p;
+    init_params(p, seed);
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    float** ps[] = {&h->w, &h->m, &h->v, &h->g};
+    for (float** q : ps)
+        if (e == cudaSuccess)
+            e = cudaMalloc(q, kParams * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&h->loss, 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&h->err, 4);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(h->w, p.data(), kParams * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemset(h->m, 0, kParams * 4);
+    if (e == cudaSuccess)
+        e = cudaMemset(h->v, 0, kParams * 4);
+    if (e == cudaSuccess)
+        e = cudaMemset(h->err, 0, 4);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        mlp_free(h);
+        return fail(BMM_ENOMEM, "mlp: allocation failed: %s", cudaGetErrorString(e));
+    }
+    *out = h;
+    return BMM_OK;
+}
+
+BMM_API int bmm_mlp_destroy(bmm_mlp* h) {
+    mlp_free(h);
+    return BMM_OK;
+}
+
+BMM_API size_t bmm_mlp_param_count(void) { return kParams; }
+
+BMM_API int bmm_mlp_get_params(bmm_mlp* h, float* params) {
+    clear_error();
+    if (!h || !params)
+        return fail(BMM_EINVAL, "mlp: null argument");
+    BMM_CUDA_TRY(cudaMemcpyAsync(params, h->w, kParams * 4, cudaMemcpyDeviceToHost, h->stream));
+    BMM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return BMM_OK;
+}
+
+BMM_API int bmm_mlp_set_params(bmm_mlp* h, const float* params) {
+    clear_error();
+    if (!h || !params)
+        return fail(BMM_EINVAL, "mlp: null argument");
+    BMM_CUDA_TRY(cudaMemcpyAsync(h->w, params, kParams * 4, cudaMemcpyHostToDevice, h->stream));
+    BMM_CUDA_TRY(cudaMemsetAsync(h->m, 0, kParams * 4, h->stream));
+    BMM_CUDA_TRY(cudaMemsetAsync(h->v, 0, kParams * 4, h->stream));
+    BMM_CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->step = 0;
+    return BMM_OK;
+}
+
+BMM_API int bmm_mlp_forward(bmm_mlp* h, const float* x, size_t rows, float* logits) {
+    clear_error();
+    if (!h || (rows && (!x || !logits)))
+        return fail(BMM_EINVAL, "mlp: null argument");
+    if (rows == 0)
+        return BMM_OK;
+    if (rows > (1u << 24))
+        return fail(BMM_EINVAL, "mlp: too many rows");
+    BMM_TRY(ensure_cap(h, rows));
+    BMM_CUDA_TRY(cudaMemcpyAsync(h->x, x, rows * kIn * 4, cudaMemcpyHostToDevice, h->stream));
+    BMM_TRY(forward_dev(h, h->x, 0, (int)rows, nullptr));
+    BMM_CUDA_TRY(cudaMemcpyAsync(logits, h->z3, rows * kOut * 4, cudaMemcpyDeviceToHost, h->stream));
+    return check_err(h);
+}
+
+BMM_API int bmm_mlp_grads(bmm_mlp* h, const float* x, const float* target, size_t rows,
+                          float* grads, float* loss) {
+    clear_error();
+    if (!h || !x || !target || !grads || rows == 0)
+        return fail(BMM_EINVAL, "mlp: null argument or no rows");
+    if (rows > (1u << 24))
+        return fail(BMM_EINVAL, "mlp: too many rows");
+    BMM_TRY(ensure_cap(h, rows));
+    BMM_CUDA_TRY(cudaMemcpyAsync(h->x, x, rows * kIn * 4, cudaMemcpyHostToDevice, h->stream));
+    BMM_CUDA_TRY(cudaMemcpyAsync(h->t, target, rows * kOut * 4, cudaMemcpyHostToDevice, h->stream));
+    BMM_CUDA_TRY(cudaMemsetAsync(h->loss, 0, 4, h->stream));
+    BMM_TRY(forward_dev(h, h->x, 0, (int)rows, nullptr));
+    BMM_TRY(backward_dev(h, h->x, 0, h->t, (int)rows));
+    BMM_CUDA_TRY(cudaMemcpyAsync(grads, h->g, kParams * 4, cudaMemcpyDeviceToHost, h->stream));
+    if (loss)
+        BMM_CUDA_TRY(cudaMemcpyAsync(loss, h->loss, 4, cudaMemcpyDeviceToHost, h->stream));
+    return check_err(h);
+}
+
+BMM_API int bmm_mlp_train(bmm_mlp* h, const float* x, const float* target, size_t rows,
+                          int steps, float* loss) {
+    clear_error();
+    if (!h || !x || !target || rows == 0 || steps < 1)
+        return fail(BMM_EINVAL, "mlp: null argument, no rows or no steps");
+    if (rows > (1u << 24))
+        return fail(BMM_EINVAL, "mlp: too many rows");
+    BMM_TRY(ensure_cap(h, rows));
+    BMM_CUDA_TRY(cudaMemcpyAsync(h->x, x, rows * kIn * 4, cudaMemcpyHostToDevice, h->stream));
+    BMM_CUDA_TRY(cudaMemcpyAsync(h->t, target, rows * kOut * 4, cudaMemcpyHostToDevice, h->stream));
+    for (int s = 0; s < steps; ++s)
+        BMM_TRY(train_step_dev(h, h->x, 0, h->t, (int)rows));
+    if (loss)
+        BMM_CUDA_TRY(cudaMemcpyAsync(loss, h->loss, 4, cudaMemcpyDeviceToHost, h->stream));
+    return check_err(h);
+}
+
+BMM_API int bmm_mlp_gemm(const float* A, const float* B, int M, int N, int K, float* C) {
+    clear_error();
+    if (!A || !B || !C || M <= 0 || N <= 0 || K <= 0)
+        return fail(BMM_EINVAL, "mlp: bad gemm arguments");
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    float *dA = nullptr, *dB = nullptr, *dC = nullptr;
+    int* derr = nullptr;
+    cudaError_t e = cudaMalloc(&dA, (size_t)M * K * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dB, (size_t)N * K * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&dC, (size_t)M * N * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&derr, 4);
+    int rc = BMM_OK;
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dA, A, (size_t)M * K * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(dB, B, (size_t)N * K * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = cudaMemset(derr, 0, 4);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        rc = fail(BMM_ECUDA, "mlp: gemm setup failed: %s", cudaGetErrorString(e));
+    }
+    if (rc == BMM_OK) {
+        GemmArgs a = gemm_args(dA, 0, K, 1, dB, 0, K, 1, M, N, K, derr);
+        a.out_f = dC;
+        a.ldo_f = N;
+        rc = gemm_launch(a, ws->stream);
+    }
+    int err = 0;
+    if (rc == BMM_OK && (cudaMemcpyAsync(C, dC, (size_t)M * N * 4, cudaMemcpyDeviceToHost,
+                                         ws->stream) != cudaSuccess ||
+                         cudaMemcpyAsync(&err, derr, 4, cudaMemcpyDeviceToHost, ws->stream) !=
+                             cudaSuccess ||
+                         cudaStreamSynchronize(ws->stream) != cudaSuccess))
+        rc = fail(BMM_ECUDA, "mlp: gemm failed: %s", cudaGetErrorString(cudaGetLastError()));
+    if (rc == BMM_OK && err)
+        rc = fail(BMM_ETIMEOUT, "mlp: a tensor-core wait timed out");
+    cudaFree(dA);
+    cudaFree(dB);
+    cudaFree(dC);
+    cudaFree(derr);
+    return rc;
+}
+
+}  // extern "C"

@@ -313,6 +313,31 @@ BMM_API int bmm_ga_crossover(size_t n, size_t parents, const uint64_t* parent_ma
                              const uint32_t* parent_weights, uint64_t* child_masks,
                              uint32_t* child_weights);
 
+/* ---- Proposal network (no reference counterpart) ---------------------------
+ * A 512 -> 256 -> 256 -> 256 ReLU MLP whose GEMMs run on the tcgen05 tensor
+ * cores (BF16 operands, FP32 accumulation in TMEM); softmax cross-entropy
+ * against target distributions; Adam (lr given, betas 0.9 / 0.999, eps 1e-8)
+ * on FP32 master parameters.  Parameters are laid out W1[256][512], b1[256],
+ * W2[256][256], b2, W3[256][256], b3 (bmm_mlp_param_count() floats).  The
+ * host-buffer entry points below are synchronous. */
+typedef struct bmm_mlp bmm_mlp;
+BMM_API int bmm_mlp_create(uint64_t seed, float learning_rate, bmm_mlp** out);
+BMM_API int bmm_mlp_destroy(bmm_mlp* h);
+BMM_API size_t bmm_mlp_param_count(void);
+BMM_API int bmm_mlp_get_params(bmm_mlp* h, float* params);
+/* also resets the Adam moments and step count */
+BMM_API int bmm_mlp_set_params(bmm_mlp* h, const float* params);
+/* x: rows x 512 inputs; logits: rows x 256 */
+BMM_API int bmm_mlp_forward(bmm_mlp* h, const float* x, size_t rows, float* logits);
+/* gradient of the mean cross-entropy against target rows (rows x 256) */
+BMM_API int bmm_mlp_grads(bmm_mlp* h, const float* x, const float* target, size_t rows,
+                          float* grads, float* loss);
+/* `steps` Adam steps on one batch; *loss: the last step's loss */
+BMM_API int bmm_mlp_train(bmm_mlp* h, const float* x, const float* target, size_t rows,
+                          int steps, float* loss);
+/* C[M][N] = bf16(A[M][K]) . bf16(B[N][K])^T in FP32 on the tensor cores */
+BMM_API int bmm_mlp_gemm(const float* A, const float* B, int M, int N, int K, float* C);
+
 #ifdef __cplusplus
 }
 #endif

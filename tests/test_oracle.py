@@ -228,3 +228,36 @@ def test_port_error_classes_match_reference():
         R.bruteforce_search(m, cols, [0, 1, 2], 4, 5)
     with pytest.raises(ValueError):
         P.bruteforce_search(m, cols, [0, 1, 2], 4, 5)
+
+
+def test_mlp_oracle_gradients_match_finite_differences():
+    """The network oracle's analytic backward pass (float64, no rounding)
+    against central differences on a sample of every parameter block."""
+    from oracle import mlp_oracle as M
+
+    rng = np.random.default_rng(3)
+    p = (rng.standard_normal(M.N_PARAMS) * 0.05).astype(np.float64)
+    X = rng.standard_normal((3, M.K_IN))
+    T = rng.random((3, M.K_OUT))
+    T /= T.sum(axis=1, keepdims=True)
+    _, g = M.loss_and_grads(p, X, T, round_bf16=False)
+    idx = np.concatenate([rng.integers(a, b, 6) for a, b in
+                          [(M.W1, M.B1), (M.B1, M.W2), (M.W2, M.B2), (M.B2, M.W3),
+                           (M.W3, M.B3), (M.B3, M.N_PARAMS)]])
+    h = 1e-6
+    for i in idx:
+        q = p.copy()
+        q[i] += h
+        lp, _ = M.loss_and_grads(q, X, T, round_bf16=False)
+        q[i] -= 2 * h
+        lm, _ = M.loss_and_grads(q, X, T, round_bf16=False)
+        fd = (lp - lm) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding_is_nearest_even():
+    from oracle import mlp_oracle as M
+
+    x = np.array([1.0, 1.00390625, 1.01171875, -2.5, 3.0e-3], np.float32)
+    # 1 + 2^-8 is a tie -> even (1.0); 1 + 3*2^-8 is a tie -> even (1 + 2^-6)
+    assert M.bf16(x).tolist() == [1.0, 1.0, 1.015625, -2.5, np.float32(0.0030059814453125)]
