@@ -66,6 +66,24 @@ class GaConfig_t(C.Structure):
                 ("target_total_weight", C.c_uint64), ("seed", C.c_uint64)]
 
 
+class GaProposal_t(C.Structure):
+    """bmm_ga_proposal."""
+
+    _fields_ = [("mode", C.c_uint32), ("queries_per_elite", C.c_uint32),
+                ("train_steps", C.c_uint32), ("reserved", C.c_uint32),
+                ("learning_rate", C.c_float), ("learned_fraction", C.c_float),
+                ("seed", C.c_uint64)]
+
+
+class GaProposalStats_t(C.Structure):
+    """bmm_ga_proposal_stats."""
+
+    _fields_ = [("tried_learned", C.c_uint64), ("improved_learned", C.c_uint64),
+                ("tried_uniform", C.c_uint64), ("improved_uniform", C.c_uint64),
+                ("examples", C.c_uint64), ("last_loss", C.c_float),
+                ("learned_fraction", C.c_float)]
+
+
 class GaMigration_t(C.Structure):
     """bmm_ga_migration (MigrationPolicy subset)."""
 
@@ -112,6 +130,8 @@ SIGNATURES = {
     "bmm_ga_best": [_vp, _sz, _u64p, _u32p, _u64p],
     "bmm_ga_population": [_vp, _sz, _u64p, _u32p, _u64p],
     "bmm_ga_destroy": [_vp],
+    "bmm_ga_set_proposal": [_vp, C.POINTER(GaProposal_t)],
+    "bmm_ga_get_proposal_stats": [_vp, C.POINTER(GaProposalStats_t)],
     "bmm_ga_eval": [_u64p, _sz, _sz, _szp, _sz, _u64p, _sz, _u32p],
     "bmm_ga_mutate": [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p, C.c_double, _u64p],
     "bmm_ga_local_improve": [_u64p, _sz, _sz, _szp, _sz, _u64p, _u32p],

@@ -1470,21 +1470,6 @@ void masks_from_device_layout(const uint64_t* in, size_t n, size_t count, uint64
 using namespace bmm;
 using namespace bmm::ga;
 
-struct bmm_ga {
-    int device = -1;
-    cudaStream_t stream = nullptr;
-    State st{};
-    int I = 0;
-    std::vector<uint32_t> intervals;  // per island export interval
-    unsigned long long gen = 0;  // generations run by the islands still active
-    int build_grid = 0, local_grid = 0;
-    size_t build_smem = 0;
-    int rank_threads = 0;
-    std::vector<void*> allocs;
-    IslandStat* h_stat = nullptr;  // pinned
-    std::vector<uint64_t> seeds;
-};
-
 namespace {
 
 int ga_alloc(bmm_ga* g, size_t bytes, void** p) {
@@ -1510,6 +1495,7 @@ void ga_free(bmm_ga* g) {
         cudaStreamSynchronize(g->stream);
     for (void* p : g->allocs)
         cudaFree(p);
+    propose_free(g);
     if (g->h_stat)
         cudaFreeHost(g->h_stat);
     if (g->stream)
@@ -1533,6 +1519,8 @@ int ga_generation(bmm_ga* g) {
     cudaStream_t s = g->stream;
     schedule_kernel<<<(I + 3) / 4, 128, 0, s>>>(st);
     build_kernel<<<g->build_grid, kBuildThreads, g->build_smem, s>>>(st, 0);
+    if (g->prop.mode != 0)
+        BMM_TRY(propose_generation(g));
     if (g->gen % 3 == 0) {  // k_local_improvement_period
         if (c.W <= kLi16MaxW)
             local_kernel<true><<<g->local_grid, kLocalThreads, local16_smem_bytes(c.N), s>>>(st);
@@ -1695,6 +1683,8 @@ BMM_API int bmm_ga_create(const uint64_t* words, size_t stride, size_t cols, con
         g->intervals[i] = ic.interval;
     }
     g->st.I = (int)islands;
+    g->cols = (uint32_t)cols;
+    g->search_grid = ws->sm_count;
     g->rank_threads = pow2_at_least(P);
     g->build_smem = build_smem_bytes(N, c.parents);
     g->build_grid = ws->sm_count * 4;
@@ -1930,6 +1920,46 @@ BMM_API int bmm_ga_population(bmm_ga* g, size_t island, uint64_t* masks, uint32_
 
 BMM_API int bmm_ga_destroy(bmm_ga* g) {
     ga_free(g);
+    return BMM_OK;
+}
+
+BMM_API int bmm_ga_set_proposal(bmm_ga* g, const bmm_ga_proposal* p) {
+    clear_error();
+    if (!g || !p)
+        return fail(BMM_EINVAL, "ga: null argument");
+    if (p->mode > 2)
+        return fail(BMM_EINVAL, "ga: proposal mode must be 0, 1 or 2");
+    if (p->mode == 0)
+        return BMM_OK;
+    if (g->prop.mode != 0)
+        return fail(BMM_EINVAL, "ga: the proposal step is already configured");
+    const Config& c = g->st.c;
+    if (c.N < 17)
+        return fail(BMM_EINVAL, "ga: the proposal step needs at least 17 window rows");
+    if (g->cols > 32767)
+        return fail(BMM_EINVAL, "ga: the proposal step needs at most 32767 columns");
+    if (p->queries_per_elite < 1 || p->queries_per_elite > 64)
+        return fail(BMM_EINVAL, "ga: queries_per_elite must be in [1, 64]");
+    if (p->mode == 1 && !(p->learning_rate > 0.f))
+        return fail(BMM_EINVAL, "ga: learning_rate must be positive");
+    if (!(p->learned_fraction >= 0.f && p->learned_fraction <= 1.f))
+        return fail(BMM_EINVAL, "ga: learned_fraction must be in [0, 1]");
+    BMM_TRY(ga_device_guard(g));
+    return propose_setup(g, (int)p->mode, (int)p->queries_per_elite, (int)p->train_steps,
+                         p->learning_rate, p->learned_fraction, p->seed);
+}
+
+BMM_API int bmm_ga_get_proposal_stats(bmm_ga* g, bmm_ga_proposal_stats* out) {
+    clear_error();
+    if (!g || !out)
+        return fail(BMM_EINVAL, "ga: null argument");
+    out->tried_learned = g->tot[0];
+    out->improved_learned = g->tot[1];
+    out->tried_uniform = g->tot[2];
+    out->improved_uniform = g->tot[3];
+    out->examples = g->examples;
+    out->last_loss = g->last_loss;
+    out->learned_fraction = g->prop.learned_frac;
     return BMM_OK;
 }
 

@@ -3,6 +3,11 @@
 
 #include "common.cuh"
 
+#include <cuda_bf16.h>
+#include <vector>
+
+struct bmm_mlp;
+
 namespace bmm {
 namespace ga {
 
@@ -84,5 +89,68 @@ struct State {
     uint32_t* Gs;               // per-CTA N x N overlap scratch for local improvement
 };
 
+// Learned proposal step (ga_propose.cu): per elite individual, qpc target
+// rows; for each, a window of 16 other rows -- chosen by the proposal network
+// or uniformly -- is searched exhaustively (packed FWHT over all 2^16
+// subsets) and an improving subset is XORed into the target row.
+struct PropBuf {
+    int mode;         // 1 learned windows (with uniform exploration), 2 uniform windows
+    int qpc;          // queries per elite individual
+    uint64_t seed;
+    float learned_frac;
+    const uint32_t* cols;  // [256] sampled columns of the row sketch
+    uint16_t* target;      // [Q] target row of each query
+    __nv_bfloat16* X;      // [Q][512] network inputs
+    float* logits;         // [Q][256]
+    float* T;              // [Q][256] training targets of improving queries
+    uint8_t* valid;        // [Q] the query found an improving subset
+    unsigned long long* counters;  // tried / improved, learned then uniform
+    __nv_bfloat16* Xb;     // replay buffer of improving examples [cap][512]
+    float* Tb;             // [cap][256]
+    int* batch_rows;       // new examples this generation, then their query indices
+};
+
+constexpr int kPropBatchCap = 4096;  // replay buffer of improving examples
+constexpr int kPropMinibatch = 512;
+
+}  // namespace ga
+}  // namespace bmm
+
+// The GA handle (bmm_ga_* in include/bmm_b200.h).
+struct bmm_ga {
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    bmm::ga::State st{};
+    int I = 0;
+    std::vector<uint32_t> intervals;  // per island export interval
+    unsigned long long gen = 0;       // generations run by the islands still active
+    int build_grid = 0, local_grid = 0;
+    size_t build_smem = 0;
+    int rank_threads = 0;
+    std::vector<void*> allocs;
+    bmm::ga::IslandStat* h_stat = nullptr;  // pinned
+    std::vector<uint64_t> seeds;
+    uint32_t cols = 0;
+    int search_grid = 0;
+    // proposal step
+    bmm::ga::PropBuf prop{};
+    unsigned long long tot[4] = {0, 0, 0, 0};  // tried / improved: learned, uniform
+    bmm_mlp* net = nullptr;
+    int train_steps = 0;
+    unsigned long long* h_counters = nullptr;  // pinned, 4
+    unsigned long long examples = 0;
+    float last_loss = 0.f;
+    double ema_tried[2] = {0, 0}, ema_improved[2] = {0, 0};  // learned, uniform (decayed)
+    int replay_head = 0, replay_fill = 0;
+};
+
+namespace bmm {
+namespace ga {
+// Runs the proposal step on the next population of the generation being
+// built (after build_kernel, before local improvement); synchronises.
+int propose_generation(bmm_ga* g);
+int propose_setup(bmm_ga* g, int mode, int qpc, int train_steps, float lr, float learned_frac,
+                  uint64_t seed);
+void propose_free(bmm_ga* g);
 }  // namespace ga
 }  // namespace bmm

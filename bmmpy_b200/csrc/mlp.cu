@@ -16,6 +16,7 @@
 // TMEM (tcgen05.ld 32x32b) and applies scale, bias, the ReLU-backward mask and
 // ReLU, writing FP32 (pre-activation) and/or BF16 (activation) outputs.
 #include "common.cuh"
+#include "mlp.cuh"
 #include "umma.cuh"
 
 #include <cmath>
@@ -24,11 +25,6 @@
 
 namespace bmm {
 namespace mlp {
-
-constexpr int kIn = 512, kHid = 256, kOut = 256;
-constexpr size_t kW1 = 0, kB1 = kW1 + (size_t)kHid * kIn, kW2 = kB1 + kHid,
-                 kB2 = kW2 + (size_t)kHid * kHid, kW3 = kB2 + kHid,
-                 kB3 = kW3 + (size_t)kOut * kHid, kParams = kB3 + kOut;
 
 constexpr int kBM = 128, kBN = 256, kBK = 64;
 constexpr int kGemmThreads = 128;
@@ -54,6 +50,8 @@ struct GemmArgs {
     long long ldo_f;
     __nv_bfloat16* out_b;    // [M][ldo_b], or null
     long long ldo_b;
+    int ksplit;              // K split over gridDim.z: partial z goes to out_f + z * split_stride
+    long long split_stride;
     int* err;
 };
 
@@ -107,8 +105,12 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     umma::fence_after_sync();
     const uint32_t tmem = tmem_slot;
     const uint32_t idesc = umma::idesc_bf16(kBM, kBN);
-    const int nk = (g.K + kBK - 1) / kBK;
-    int kc = 0;
+    const int nk_all = (g.K + kBK - 1) / kBK;
+    const int per = (nk_all + g.ksplit - 1) / g.ksplit;
+    const int kbeg = blockIdx.z * per;
+    const int nk = min(nk_all, kbeg + per);
+    float* out_f = g.out_f ? g.out_f + (long long)blockIdx.z * g.split_stride : nullptr;
+    int kc = kbeg;
     for (; kc < nk; ++kc) {
         stage(sA, kBM, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M, kc * kBK, g.K);
         stage(sB, kBN, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N, kc * kBK, g.K);
@@ -121,17 +123,18 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
             for (int s = 0; s < kBK / 16; ++s) {
                 const uint64_t da = umma::smem_desc(a0 + s * 256, 128, (kBK / 8) * 128);
                 const uint64_t db = umma::smem_desc(b0 + s * 256, 128, (kBK / 8) * 128);
-                umma::mma_bf16(tmem, da, db, idesc, (kc > 0 || s > 0) ? 1u : 0u);
+                umma::mma_bf16(tmem, da, db, idesc, (kc > kbeg || s > 0) ? 1u : 0u);
             }
             umma::commit(umma::smem_u32(&mbar));
         }
-        if (!umma::mbar_wait(umma::smem_u32(&mbar), kc & 1, kWaitLimit))
+        if (!umma::mbar_wait(umma::smem_u32(&mbar), (kc - kbeg) & 1, kWaitLimit))
             s_fail = 1;
         __syncthreads();
         if (s_fail)
             break;
     }
     umma::fence_after_sync();
+    const bool empty = kbeg >= nk;  // this split has no K chunk: its partial is zero
     if (!s_fail) {
         const int m = m0 + warp * 32 + lane;
         for (int c = 0; c < kBN / 32; ++c) {
@@ -139,6 +142,10 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
             umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), v);
             if (m >= g.M)
                 continue;
+            if (empty)
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    v[i] = 0.f;
 #pragma unroll
             for (int i = 0; i < 32; ++i) {
                 const int n = n0 + c * 32 + i;
@@ -149,8 +156,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
                     val += g.bias[n];
                 if (g.relu_mask && !(g.relu_mask[(long long)m * g.ldm + n] > 0.f))
                     val = 0.f;
-                if (g.out_f)
-                    g.out_f[(long long)m * g.ldo_f + n] = val;
+                if (out_f)
+                    out_f[(long long)m * g.ldo_f + n] = val;
                 if (g.out_b)
                     g.out_b[(long long)m * g.ldo_b + n] =
                         __float2bfloat16_rn(g.relu ? fmaxf(val, 0.f) : val);
@@ -160,7 +167,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
         if (tid == 0)
             atomicExch(g.err, 1);
         // let the MMAs in flight finish (bounded) before the TMEM is released
-        umma::mbar_wait(umma::smem_u32(&mbar), kc & 1, kWaitLimit);
+        umma::mbar_wait(umma::smem_u32(&mbar), (kc - kbeg) & 1, kWaitLimit);
     }
     umma::fence_before_sync();
     __syncthreads();
@@ -227,6 +234,18 @@ __global__ void colsum_kernel(const float* __restrict__ d, int rows, float* __re
     out[n] = s;
 }
 
+// out[i] = sum over z < splits of part[z * n + i], in z order (deterministic).
+__global__ void split_reduce_kernel(const float* __restrict__ part, int splits, size_t n,
+                                    float* __restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n)
+        return;
+    float s = 0.f;
+    for (int z = 0; z < splits; ++z)
+        s += part[(size_t)z * n + i];
+    out[i] = s;
+}
+
 // Adam (Kingma & Ba) with bias correction on the FP32 master parameters.
 __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                             const float* __restrict__ grad, size_t n, float lr, float b1, float b2,
@@ -248,32 +267,6 @@ __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float*
 using namespace bmm;
 using namespace bmm::mlp;
 
-// Network state: parameters, Adam moments, gradients and activation scratch
-// for up to `cap` rows, all device-resident.
-struct bmm_mlp {
-    int device = -1;
-    cudaStream_t stream = nullptr;
-    float* w = nullptr;  // kParams
-    float* m = nullptr;
-    float* v = nullptr;
-    float* g = nullptr;
-    long long step = 0;
-    float lr = 1e-3f, b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    size_t cap = 0;
-    float* z1 = nullptr;  // [cap][256] pre-activations
-    float* z2 = nullptr;
-    float* z3 = nullptr;  // logits
-    __nv_bfloat16* h1 = nullptr;
-    __nv_bfloat16* h2 = nullptr;
-    float* dz3 = nullptr;
-    float* dz2 = nullptr;
-    float* dz1 = nullptr;
-    float* x = nullptr;  // [cap][512] staging for host inputs
-    float* t = nullptr;  // [cap][256] targets
-    float* loss = nullptr;
-    int* err = nullptr;
-};
-
 namespace {
 
 int gemm_launch(const GemmArgs& a, cudaStream_t s) {
@@ -285,7 +278,7 @@ int gemm_launch(const GemmArgs& a, cudaStream_t s) {
                                           (int)kGemmSmem));
         attr_dev = dev;
     }
-    dim3 grid((a.M + kBM - 1) / kBM, (a.N + kBN - 1) / kBN);
+    dim3 grid((a.M + kBM - 1) / kBM, (a.N + kBN - 1) / kBN, a.ksplit > 1 ? a.ksplit : 1);
     gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(a);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -309,8 +302,25 @@ GemmArgs gemm_args(const void* A, int a_bf16, long long lda_m, long long lda_k, 
     a.N = N;
     a.K = K;
     a.scale = 1.f;
+    a.ksplit = 1;
     a.err = err;
     return a;
+}
+
+// Weight gradient dW[M][N] = A^T-like product with K = batch rows, split over
+// K into `part` (ksplit partials of M * N) and reduced in a fixed order.
+int gemm_wgrad(GemmArgs a, float* out, float* part, cudaStream_t s) {
+    const int nk = (a.K + kBK - 1) / kBK;
+    const int splits = std::max(1, std::min(nk, 16));
+    const size_t n = (size_t)a.M * a.N;
+    a.ksplit = splits;
+    a.out_f = splits > 1 ? part : out;
+    a.ldo_f = a.N;
+    a.split_stride = (long long)n;
+    BMM_TRY(gemm_launch(a, s));
+    if (splits > 1)
+        split_reduce_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(part, splits, n, out);
+    return BMM_OK;
 }
 
 int check_err(bmm_mlp* h) {
@@ -322,7 +332,9 @@ int check_err(bmm_mlp* h) {
     return BMM_OK;
 }
 
-int ensure_cap(bmm_mlp* h, size_t rows) {
+}  // namespace
+
+int bmm::mlp::ensure_cap(bmm_mlp* h, size_t rows) {
     if (rows <= h->cap)
         return BMM_OK;
     size_t cap = std::max<size_t>(rows, 256);
@@ -355,7 +367,6 @@ int ensure_cap(bmm_mlp* h, size_t rows) {
     return BMM_OK;
 }
 
-}  // namespace
 
 namespace bmm {
 namespace mlp {
@@ -393,9 +404,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     xent_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(h->z3, T, h->dz3, h->loss, rows);
     // dW3 = dZ3^T H2, db3
     GemmArgs a = gemm_args(h->dz3, 0, 1, kOut, h->h2, 1, 1, kHid, kOut, kHid, rows, h->err);
-    a.out_f = h->g + kW3;
-    a.ldo_f = kHid;
-    BMM_TRY(gemm_launch(a, s));
+    BMM_TRY(gemm_wgrad(a, h->g + kW3, h->part, s));
     colsum_kernel<<<1, 256, 0, s>>>(h->dz3, rows, h->g + kB3);
     // dZ2 = (dZ3 W3) * (Z2 > 0)
     a = gemm_args(h->dz3, 0, kOut, 1, h->w + kW3, 0, 1, kHid, rows, kHid, kOut, h->err);
@@ -406,9 +415,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     BMM_TRY(gemm_launch(a, s));
     // dW2 = dZ2^T H1, db2
     a = gemm_args(h->dz2, 0, 1, kHid, h->h1, 1, 1, kHid, kHid, kHid, rows, h->err);
-    a.out_f = h->g + kW2;
-    a.ldo_f = kHid;
-    BMM_TRY(gemm_launch(a, s));
+    BMM_TRY(gemm_wgrad(a, h->g + kW2, h->part, s));
     colsum_kernel<<<1, 256, 0, s>>>(h->dz2, rows, h->g + kB2);
     // dZ1 = (dZ2 W2) * (Z1 > 0)
     a = gemm_args(h->dz2, 0, kHid, 1, h->w + kW2, 0, 1, kHid, rows, kHid, kHid, h->err);
@@ -419,9 +426,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     BMM_TRY(gemm_launch(a, s));
     // dW1 = dZ1^T X (N = 512: two column tiles), db1
     a = gemm_args(h->dz1, 0, 1, kHid, X, x_bf16, 1, kIn, kHid, kIn, rows, h->err);
-    a.out_f = h->g + kW1;
-    a.ldo_f = kIn;
-    BMM_TRY(gemm_launch(a, s));
+    BMM_TRY(gemm_wgrad(a, h->g + kW1, h->part, s));
     colsum_kernel<<<1, 256, 0, s>>>(h->dz1, rows, h->g + kB1);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -481,13 +486,13 @@ void mlp_free(bmm_mlp* h) {
     if (h->stream)
         cudaStreamSynchronize(h->stream);
     float* fs[] = {h->w, h->m, h->v, h->g, h->z1, h->z2, h->z3, h->dz3, h->dz2, h->dz1, h->x,
-                   h->t, h->loss};
+                   h->t, h->loss, h->part};
     for (float* p : fs)
         cudaFree(p);
     cudaFree(h->h1);
     cudaFree(h->h2);
     cudaFree(h->err);
-    if (h->stream)
+    if (h->stream && h->owns_stream)
         cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -509,16 +514,41 @@ BMM_API int bmm_mlp_create(uint64_t seed, float learning_rate, bmm_mlp** out) {
         return st;
     if (ws->sm_count <= 0)
         return fail(BMM_ENODEV, "mlp: no CUDA device");
+    bmm_mlp* h = nullptr;
+    BMM_TRY(bmm::mlp::create(seed, learning_rate, nullptr, &h));
+    *out = h;
+    return BMM_OK;
+}
+
+}  // extern "C"
+
+namespace bmm {
+namespace mlp {
+
+int create(uint64_t seed, float learning_rate, cudaStream_t stream, bmm_mlp** out) {
+    *out = nullptr;
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
     bmm_mlp* h = new bmm_mlp();
     h->device = ws->device;
     h->lr = learning_rate;
     std::vector<float> p;
     init_params(p, seed);
-    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    cudaError_t e = cudaSuccess;
+    if (stream) {
+        h->stream = stream;
+        h->owns_stream = false;
+    } else {
+        e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    }
     float** ps[] = {&h->w, &h->m, &h->v, &h->g};
     for (float** q : ps)
         if (e == cudaSuccess)
             e = cudaMalloc(q, kParams * 4);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&h->part, (size_t)16 * kHid * kIn * 4);
     if (e == cudaSuccess)
         e = cudaMalloc(&h->loss, 4);
     if (e == cudaSuccess)
@@ -539,6 +569,13 @@ BMM_API int bmm_mlp_create(uint64_t seed, float learning_rate, bmm_mlp** out) {
     *out = h;
     return BMM_OK;
 }
+
+void destroy(bmm_mlp* h) { mlp_free(h); }
+
+}  // namespace mlp
+}  // namespace bmm
+
+extern "C" {
 
 BMM_API int bmm_mlp_destroy(bmm_mlp* h) {
     mlp_free(h);

@@ -35,7 +35,7 @@ from .matrix import RowWindow
 __all__ = [
     "StopCriteria", "RunStats", "MigrationPolicy", "IslandSpec", "IslandSnapshot",
     "IslandModelSnapshot", "GeneticAlgorithmConfig", "IslandModelConfig", "OverflowPolicy",
-    "GeneticAlgorithm", "IslandModel",
+    "GeneticAlgorithm", "IslandModel", "ProposalConfig",
 ]
 
 
@@ -226,11 +226,42 @@ def _individual(masks: np.ndarray, weights: np.ndarray) -> list[Candidate]:
     return [Candidate([int(w) for w in masks[i]], int(weights[i])) for i in range(len(weights))]
 
 
+class ProposalConfig:
+    """Learned proposal step (no bmmpy counterpart; bmm_ga_proposal).
+
+    mode: "off" (the reference GA), "learned" (windows of 16 rows drawn from
+    the proposal network's scores, with uniform exploration, exhaustively
+    searched and trained on the improving subsets) or "uniform" (uniform
+    windows only, the ablation without the network)."""
+
+    __slots__ = ("mode", "queries_per_elite", "train_steps", "learning_rate",
+                 "learned_fraction", "seed")
+
+    def __init__(self, mode: str = "off", queries_per_elite: int = 2, train_steps: int = 2,
+                 learning_rate: float = 1e-3, learned_fraction: float = 0.5,
+                 seed: int = 1) -> None:
+        if mode not in ("off", "learned", "uniform"):
+            raise ValueError(f"Unsupported proposal mode: {mode!r}")
+        self.mode = mode
+        self.queries_per_elite = queries_per_elite
+        self.train_steps = train_steps
+        self.learning_rate = learning_rate
+        self.learned_fraction = learned_fraction
+        self.seed = seed
+
+    def native(self) -> N.GaProposal_t:
+        return N.GaProposal_t({"off": 0, "learned": 1, "uniform": 2}[self.mode],
+                              int(self.queries_per_elite), int(self.train_steps), 0,
+                              float(self.learning_rate), float(self.learned_fraction),
+                              int(self.seed) & 0xFFFFFFFFFFFFFFFF)
+
+
 class _Engine:
     """One device run of `islands` islands (the bmm_ga handle)."""
 
     def __init__(self, window: RowWindow, configs: Sequence[GeneticAlgorithmConfig],
-                 migration: Sequence[MigrationPolicy] | None) -> None:
+                 migration: Sequence[MigrationPolicy] | None,
+                 proposal: ProposalConfig | None = None) -> None:
         m = window.matrix
         self.words = np.ascontiguousarray(m.words)
         self.win = np.ascontiguousarray(window.index_array(), dtype=np.uintp)
@@ -249,6 +280,15 @@ class _Engine:
                                       C.byref(h)))
         self.h = h
         self.lock = threading.Lock()
+        if proposal is not None and proposal.mode != "off":
+            cfg = proposal.native()
+            N.check(N.lib().bmm_ga_set_proposal(self.h, C.byref(cfg)))
+
+    def proposal_stats(self) -> dict:
+        out = N.GaProposalStats_t()
+        with self.lock:
+            N.check(N.lib().bmm_ga_get_proposal_stats(self.h, C.byref(out)))
+        return {k: getattr(out, k) for k, _ in out._fields_}
 
     def run(self, generations: int, check_every: int = 1) -> tuple[int, bool]:
         ran = C.c_uint64(0)
@@ -311,14 +351,16 @@ class GeneticAlgorithm:
     __slots__ = ("population_size", "elite_count", "tournament_size", "num_parents",
                  "num_offspring", "enable_catastrophe", "catastrophe_threshold",
                  "catastrophe_survival_rate", "mutation_rate", "max_generations",
-                 "max_stale_generations", "target_total_weight", "seed", "_engine", "_done")
+                 "max_stale_generations", "target_total_weight", "seed", "_engine", "_done",
+                 "proposal")
 
     def __init__(self, *, population_size: int = 300, elite_count: int = 3,
                  tournament_size: int = 3, num_parents: int = 2, num_offspring: int = 1,
                  enable_catastrophe: bool = False, catastrophe_threshold: int = 30,
                  catastrophe_survival_rate: float = 0.2, mutation_rate: float = 0.3,
                  max_generations: int | None = None, max_stale_generations: int | None = None,
-                 target_total_weight: int | None = None, seed: int = 0) -> None:
+                 target_total_weight: int | None = None, seed: int = 0,
+                 proposal: ProposalConfig | None = None) -> None:
         self.population_size = population_size
         self.elite_count = elite_count
         self.tournament_size = tournament_size
@@ -332,6 +374,7 @@ class GeneticAlgorithm:
         self.max_stale_generations = max_stale_generations
         self.target_total_weight = target_total_weight
         self.seed = seed
+        self.proposal = proposal
         self._engine: _Engine | None = None
         self._done = False
 
@@ -367,7 +410,7 @@ class GeneticAlgorithm:
                 "GeneticAlgorithm::initialize: population_size must be greater than zero")
         if self._engine is not None:
             self._engine.close()
-        self._engine = _Engine(window, [self._config()], None)
+        self._engine = _Engine(window, [self._config()], None, self.proposal)
         self._done = bool(self._engine.stats(0).done)
 
     def step(self) -> None:
@@ -420,7 +463,8 @@ class IslandModel:
     """
 
     __slots__ = ("island_count", "channel_capacity", "overflow_policy", "_specs", "_configs",
-                 "_engine", "_thread", "_running", "_stop", "_error", "_initialized")
+                 "_engine", "_thread", "_running", "_stop", "_error", "_initialized",
+                 "_proposal")
 
     def __init__(self, *, islands: Sequence[IslandSpec],
                  ga_configs: Sequence[GeneticAlgorithmConfig] | None = None,
@@ -430,7 +474,8 @@ class IslandModel:
                  mutation_rate: float = 0.3, max_generations: int | None = None,
                  max_stale_generations: int | None = None,
                  target_total_weight: int | None = None, seed: int = 0, seed_stride: int = 1,
-                 channel_capacity: int = 256, overflow_policy="drop_oldest") -> None:
+                 channel_capacity: int = 256, overflow_policy="drop_oldest",
+                 proposal: ProposalConfig | None = None) -> None:
         island_list = list(islands)
         if not island_list:
             raise ValueError("IslandModel requires at least one island")
@@ -475,6 +520,7 @@ class IslandModel:
         self._stop = threading.Event()
         self._error: BaseException | None = None
         self._initialized = False
+        self._proposal = proposal
 
     def __repr__(self) -> str:
         return (f"IslandModel(island_count={self.island_count}, "
@@ -490,7 +536,8 @@ class IslandModel:
         _check_window(window)
         if self._engine is not None:
             self._engine.close()
-        self._engine = _Engine(window, self._configs, [s.migration for s in self._specs])
+        self._engine = _Engine(window, self._configs, [s.migration for s in self._specs],
+                               self._proposal)
         self._stop.clear()
         self._initialized = True
 
@@ -566,6 +613,10 @@ class IslandModel:
             snap.islands.append(isl)
         snap.best_score = best if best is not None else 0
         return snap
+
+    def proposal_stats(self) -> dict:
+        """Counters of the learned proposal step (no bmmpy counterpart)."""
+        return self._engine.proposal_stats() if self._engine else {}
 
     def run_to_completion(self, window: RowWindow) -> list[Candidate]:
         self.initialize(window)

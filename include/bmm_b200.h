@@ -295,6 +295,38 @@ BMM_API int bmm_ga_best(bmm_ga* g, size_t island, uint64_t* masks, uint32_t* wei
 BMM_API int bmm_ga_population(bmm_ga* g, size_t island, uint64_t* masks, uint32_t* weights,
                               uint64_t* fitness);
 BMM_API int bmm_ga_destroy(bmm_ga* g);
+/* Learned proposal step (no reference counterpart), run after each
+ * generation's population is built: for queries_per_elite target rows of
+ * every elite individual (the islands' best, carried into the next
+ * population), a window of 16 other rows is searched exhaustively (all 2^16
+ * XOR subsets, packed FWHT) and an improving subset is applied, re-scored
+ * exactly.  mode 1 draws the windows from the proposal network's scores
+ * (Gumbel-top-16) with probability learned_fraction -- adapted each
+ * generation towards whichever of learned and uniform windows improves more
+ * often -- and uniformly otherwise, and trains the network (train_steps Adam
+ * steps per generation) on the improving subsets; mode 2 uses uniform windows
+ * only; mode 0 (default) is the reference GA.  Needs 17..256 window rows and
+ * at most 32767 columns.  Set once, before running. */
+typedef struct bmm_ga_proposal {
+    uint32_t mode;
+    uint32_t queries_per_elite; /* 1..64 */
+    uint32_t train_steps;
+    uint32_t reserved;
+    float learning_rate;
+    float learned_fraction;
+    uint64_t seed;
+} bmm_ga_proposal;
+typedef struct bmm_ga_proposal_stats {
+    uint64_t tried_learned;
+    uint64_t improved_learned;
+    uint64_t tried_uniform;
+    uint64_t improved_uniform;
+    uint64_t examples;      /* training examples used */
+    float last_loss;        /* cross-entropy of the last training step */
+    float learned_fraction; /* current share of learned windows */
+} bmm_ga_proposal_stats;
+BMM_API int bmm_ga_set_proposal(bmm_ga* g, const bmm_ga_proposal* p);
+BMM_API int bmm_ga_get_proposal_stats(bmm_ga* g, bmm_ga_proposal_stats* out);
 /* Operators on one individual, through the same device code as the
  * generation kernels.  eval: internal::eval_cand_weight
  * (genetic_algorithm_internal.hpp:41-103) of `count` masks.  mutate:
