@@ -178,9 +178,9 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
 }
 
 // Softmax cross-entropy against target distributions: warp per row.
-// dlogits = (softmax - target) / rows; *loss += -sum(target * log softmax) / rows.
+// dlogits = (softmax - target) / rows; row_loss[r] = -sum(target * log softmax) / rows.
 __global__ void xent_kernel(const float* __restrict__ logits, const float* __restrict__ target,
-                            float* __restrict__ dlogits, float* loss, int rows) {
+                            float* __restrict__ dlogits, float* row_loss, int rows) {
     const int lane = threadIdx.x & 31;
     const int r = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (r >= rows)
@@ -219,8 +219,25 @@ __global__ void xent_kernel(const float* __restrict__ logits, const float* __res
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1)
         l += __shfl_xor_sync(kFull, l, o);
-    if (lane == 0 && loss)
-        atomicAdd(loss, l * inv);
+    if (lane == 0)
+        row_loss[r] = l * inv;
+}
+
+// *loss = sum of row_loss in row order (one CTA, fixed reduction tree).
+__global__ void loss_sum_kernel(const float* __restrict__ row_loss, int rows, float* loss) {
+    __shared__ float part[256];
+    float s = 0.f;
+    for (int r = threadIdx.x; r < rows; r += blockDim.x)
+        s += row_loss[r];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w)
+            part[threadIdx.x] += part[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        *loss = part[0];
 }
 
 // Column sums of a [rows][256] matrix (bias gradients).
@@ -338,7 +355,7 @@ int bmm::mlp::ensure_cap(bmm_mlp* h, size_t rows) {
     if (rows <= h->cap)
         return BMM_OK;
     size_t cap = std::max<size_t>(rows, 256);
-    float** fs[] = {&h->z1, &h->z2, &h->z3, &h->dz3, &h->dz2, &h->dz1, &h->t};
+    float** fs[] = {&h->z1, &h->z2, &h->z3, &h->dz3, &h->dz2, &h->dz1, &h->t, &h->row_loss};
     for (float** p : fs) {
         cudaFree(*p);
         *p = nullptr;
@@ -401,7 +418,8 @@ int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) 
 // targets T [rows][256]) into h->g; the loss is added to *h->loss.
 int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows) {
     cudaStream_t s = h->stream;
-    xent_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(h->z3, T, h->dz3, h->loss, rows);
+    xent_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(h->z3, T, h->dz3, h->row_loss, rows);
+    loss_sum_kernel<<<1, 256, 0, s>>>(h->row_loss, rows, h->loss);
     // dW3 = dZ3^T H2, db3
     GemmArgs a = gemm_args(h->dz3, 0, 1, kOut, h->h2, 1, 1, kHid, kOut, kHid, rows, h->err);
     BMM_TRY(gemm_wgrad(a, h->g + kW3, h->part, s));
@@ -486,7 +504,7 @@ void mlp_free(bmm_mlp* h) {
     if (h->stream)
         cudaStreamSynchronize(h->stream);
     float* fs[] = {h->w, h->m, h->v, h->g, h->z1, h->z2, h->z3, h->dz3, h->dz2, h->dz1, h->x,
-                   h->t, h->loss, h->part};
+                   h->t, h->loss, h->part, h->row_loss};
     for (float* p : fs)
         cudaFree(p);
     cudaFree(h->h1);

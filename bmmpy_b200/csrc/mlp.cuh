@@ -41,6 +41,7 @@ struct bmm_mlp {
     float* x = nullptr;  // [cap][512] staging for host inputs
     float* t = nullptr;  // [cap][256] targets
     float* loss = nullptr;
+    float* row_loss = nullptr;  // [cap]
     float* part = nullptr;  // split-K partials of the weight gradients (16 x 256 x 512)
     int* err = nullptr;
 };
