@@ -26,6 +26,17 @@ Multi-GPU: one process per GPU (torchrun); rank r runs the same workload on
 its own instance (seed 1 + r), no collective on the data path ("weak").
 ``--impl reference`` times the reference CPU implementation instead (rank 0
 only).
+
+``--workload ga`` (1 GPU) measures the island-model GA instead: the planted
+256 x 8192 matrix (density 0.01, 5000 scrambles, seed 7), 64 islands x 256,
+ring migration every 20 generations, stop at the planted weight or the
+wall-clock cap; the plain GA (the reference's algorithm), the proposal step
+with uniform windows, and the learned proposal step, over --seeds seeds.
+Reports generations/s and, per seed, the wall-clock each variant needs to
+reach the best weight the plain GA reaches within the cap (time-to-threshold;
+no variant reaches the planted weight within the cap).  With --impl reference
+the reference IslandModel (one thread per island, host cores) runs the same
+configuration under the same cap.
 """
 
 from __future__ import annotations
@@ -204,6 +215,128 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+GA = dict(rows=256, cols=8192, p=0.01, seed=7, scrambles=5000, interval=20)
+
+
+def _ga_first_time(trace, threshold):
+    for t, g, best in trace:
+        if best <= threshold:
+            return t, g
+    return None, None
+
+
+def run_ga(args):
+    """Time-to-threshold of the plain / uniform-window / learned GA."""
+    if args.impl == "reference":
+        return run_ga_reference(args)
+    import bmmpy_b200 as bmm
+    from bmmpy_b200.ga import ProposalConfig
+    from bmmpy_b200.workloads import gen_instance
+
+    m, planted = gen_instance(GA["rows"], GA["cols"], GA["p"], GA["seed"], GA["scrambles"])
+    win = m.row_window(list(range(GA["rows"])))
+
+    def spec(i):
+        sp = bmm.IslandSpec()
+        sp.island_id = i
+        sp.migration.interval_generations = GA["interval"]
+        sp.migration.import_count = 1
+        return sp
+
+    runs = {}
+    for seed in range(1, args.seeds + 1):
+        for mode in ("off", "uniform", "learned"):
+            prop = ProposalConfig(mode, queries_per_elite=32, train_steps=1, seed=seed)
+            model = bmm.IslandModel(islands=[spec(i) for i in range(args.islands)],
+                                    population_size=args.population,
+                                    target_total_weight=planted, max_generations=10 ** 9,
+                                    seed=1000 * seed, proposal=prop)
+            t0 = time.perf_counter()
+            model.initialize(win)
+            eng = model._engine
+            trace = [(time.perf_counter() - t0, 0, min(int(eng.stats(i).best_score)
+                                                    for i in range(args.islands)))]
+            gens = 0
+            while time.perf_counter() - t0 < args.cap:
+                ran, done = eng.run(1)
+                gens += ran
+                best = min(int(eng.stats(i).best_score) for i in range(args.islands))
+                trace.append((time.perf_counter() - t0, gens, best))
+                if done:
+                    break
+            elapsed = time.perf_counter() - t0
+            runs[(mode, seed)] = {"trace": trace, "gens": gens, "elapsed": elapsed,
+                                  "best": trace[-1][2],
+                                  "proposal": model.proposal_stats() if mode != "off" else None}
+            del model, eng
+    seeds_out = []
+    for seed in range(1, args.seeds + 1):
+        plain = runs[("off", seed)]
+        thr = plain["best"]
+        entry = {"seed": seed, "threshold_plain_best": thr}
+        for mode in ("off", "uniform", "learned"):
+            r = runs[(mode, seed)]
+            t, g = _ga_first_time(r["trace"], thr)
+            entry[mode] = {"best_at_cap": r["best"], "generations": r["gens"],
+                           "gens_per_s": r["gens"] / r["elapsed"], "time_to_threshold_s": t,
+                           "gens_to_threshold": g, "reached_planted": r["best"] <= planted}
+            if r["proposal"]:
+                entry[mode]["proposal"] = r["proposal"]
+        ulr = runs[("uniform", seed)]["best"]
+        tl, _ = _ga_first_time(runs[("learned", seed)]["trace"], ulr)
+        tu, _ = _ga_first_time(runs[("uniform", seed)]["trace"], ulr)
+        entry["learned_vs_uniform"] = {"threshold_uniform_best": ulr, "uniform_s": tu,
+                                       "learned_s": tl}
+        seeds_out.append(entry)
+    speedups = [e["off"]["time_to_threshold_s"] / e["learned"]["time_to_threshold_s"]
+                for e in seeds_out if e["learned"]["time_to_threshold_s"]]
+    line = {
+        "metric": "time-to-threshold speed-up, learned vs plain GA (threshold: the plain GA's "
+                  "best weight within the cap)",
+        "value": statistics.median(speedups) if speedups else None, "unit": "x",
+        "higher_is_better": True, "n_gpus": 1, "dtype": "u64 (+bf16 network)",
+        "data": "synthetic planted matrix (xorshift64 seed 7)", "vs_baseline": None,
+        "config": {"workload": "GA island model on a planted 256x8192 matrix (density 0.01, "
+                               "5000 scrambles, seed 7)", "islands": args.islands,
+                   "population": args.population, "migration": "ring, every 20 generations",
+                   "cap_s": args.cap, "planted_weight": planted,
+                   "proposal": "32 queries per elite, 16-row windows, 1 Adam step/generation"},
+        "seeds": seeds_out,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ga_reference(args):
+    from oracle.oracle import port, ref
+
+    R = ref()
+    if R is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+        return 0
+    P = port()
+    words, planted = P.gen_instance(GA["rows"], GA["cols"], GA["p"], GA["seed"], GA["scrambles"])
+    out = []
+    for seed in range(1, args.seeds + 1):
+        best, secs = R.island_run(words, GA["cols"], list(range(GA["rows"])), args.islands,
+                                  args.population, GA["interval"], seed, 10 ** 9, planted,
+                                  args.cap)
+        out.append({"seed": seed, "best_at_cap": best, "seconds": secs,
+                    "reached_planted": best <= planted})
+    line = {"impl": "reference", "metric": "GA best weight within the cap (reference IslandModel)",
+            "value": statistics.median([o["best_at_cap"] for o in out]), "unit": "weight",
+            "higher_is_better": False, "n_gpus": 0,
+            "config": {"workload": "GA island model on a planted 256x8192 matrix",
+                       "islands": args.islands, "population": args.population,
+                       "migration": "shared pool every 20 generations (reference channel)",
+                       "cap_s": args.cap, "planted_weight": planted,
+                       "cores": os.cpu_count()},
+            "seeds": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -211,8 +344,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="gray", choices=["gray", "ga"])
+    ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
+    ap.add_argument("--seeds", type=int, default=2, help="GA: seeds per variant")
+    ap.add_argument("--islands", type=int, default=64)
+    ap.add_argument("--population", type=int, default=256)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.workload == "ga":
+        return run_ga(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -1927,8 +1927,8 @@ BMM_API int bmm_ga_set_proposal(bmm_ga* g, const bmm_ga_proposal* p) {
     clear_error();
     if (!g || !p)
         return fail(BMM_EINVAL, "ga: null argument");
-    if (p->mode > 2)
-        return fail(BMM_EINVAL, "ga: proposal mode must be 0, 1 or 2");
+    if (p->mode > 3)
+        return fail(BMM_EINVAL, "ga: proposal mode must be 0, 1, 2 or 3");
     if (p->mode == 0)
         return BMM_OK;
     if (g->prop.mode != 0)

@@ -94,12 +94,14 @@ struct State {
 // or uniformly -- is searched exhaustively (packed FWHT over all 2^16
 // subsets) and an improving subset is XORed into the target row.
 struct PropBuf {
-    int mode;         // 1 learned windows (with uniform exploration), 2 uniform windows
+    int mode;         // 1 learned windows (with uniform exploration), 2 uniform windows,
+                      // 3 the 16 rows of smallest pairwise weight change
     int qpc;          // queries per elite individual
     uint64_t seed;
     float learned_frac;
     const uint32_t* cols;  // [256] sampled columns of the row sketch
     uint16_t* target;      // [Q] target row of each query
+    uint16_t* perm;        // [Q][256] row at each rank position
     __nv_bfloat16* X;      // [Q][512] network inputs
     float* logits;         // [Q][256]
     float* T;              // [Q][256] training targets of improving queries

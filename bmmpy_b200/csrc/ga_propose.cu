@@ -3,17 +3,17 @@
 //
 // Per generation, for qpc target rows i of every elite individual (the
 // islands' best, copied into the next population):
-//  1. features_kernel: the network input of (individual, i): for every other
-//     row j the exact relative weight change (w_j - 2 popc(r_i & r_j)) / w_i
-//     that XORing r_j into r_i would cause, then the ±1 bits of r_i's
-//     256-column sketch (r_i sampled at 256 fixed columns);
-//  2. the proposal network (mlp.cu, tcgen05 GEMMs) scores every row j;
+//  1. features_kernel: the network input of (individual, i): the exact
+//     relative weight change d_j = (w_j - 2 popc(r_i & r_j)) / w_i that
+//     XORing r_j into r_i would cause, for the rows j ranked by d_j, then the
+//     ±1 bits of r_i's 256-column sketch (r_i sampled at 256 fixed columns);
+//  2. the proposal network (mlp.cu, tcgen05 GEMMs) scores every rank position;
 //  3. search_kernel: a window of 16 rows j != i is drawn -- Gumbel-top-16 of
-//     the scores (learned), or uniformly -- and the exact best subset of the
+//     the position scores (learned), or uniformly -- and the exact best subset of the
 //     window to XOR into r_i is found by the packed FWHT over all 2^16 subsets
 //     (target_item.cuh); an improving subset is applied (row, mask and exact
 //     weight) and becomes a training example whose target spreads the mass
-//     evenly over the subset's rows;
+//     evenly over the rank positions of the subset's rows;
 //  4. the improving examples, compacted in query order, train the network
 //     with `train_steps` Adam steps.
 // The share of learned windows adapts to the measured success rates of
@@ -60,11 +60,18 @@ __device__ __forceinline__ uint32_t query_slot(const State& st, const PropBuf& p
 }
 
 // CTA (256 threads) per query: exact overlaps popc(r_i & r_j) for every row
-// j (warp per j, lanes over words), the network input
-// [(w_j - 2 ov_ij) / w_i for j < 256 | ±1 sketch bits of r_i], and the target.
+// j (warp per j, lanes over words) give the pairwise weight changes
+// d_j = (w_j - 2 ov_ij) / w_i; the rows are ranked by (d_j, j) (bitonic sort;
+// row i and rows past N last) and the network input is
+// [d of the rank-k row for k < 256 | ±1 sketch bits of r_i]; perm[q][k] is
+// the rank-k row, so the network scores rank positions.
+constexpr float kNoRow = 1e30f;
+
 __global__ void __launch_bounds__(256) features_kernel(State st, PropBuf pb,
                                                        unsigned long long gen) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ float sd[256];
+    __shared__ uint16_t sj[256];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
     const int N = st.c.N, W = st.c.W;
     const uint64_t Q = (uint64_t)st.I * st.c.E * pb.qpc;
     for (uint64_t q = blockIdx.x; q < Q; q += gridDim.x) {
@@ -76,13 +83,12 @@ __global__ void __launch_bounds__(256) features_kernel(State st, PropBuf pb,
         const uint64_t* R = p.rows + (size_t)cs * N * W;
         const uint32_t* wt = p.wts + (size_t)cs * N;
         const int i = (int)(qhash(pb.seed, gen, q, 0x7a) % (uint64_t)N);
-        if (threadIdx.x == 0)
+        if (tid == 0)
             pb.target[q] = (uint16_t)i;
         const float wi = (float)max(wt[i], 1u);
-        __nv_bfloat16* x = pb.X + q * 512;
         const uint64_t* ri = R + (size_t)i * W;
         for (int j = warp; j < 256; j += nw) {
-            float d = 0.f;
+            float d = kNoRow;
             if (j < N && j != i) {
                 uint32_t ov = 0;
                 const uint64_t* rj = R + (size_t)j * W;
@@ -93,14 +99,35 @@ __global__ void __launch_bounds__(256) features_kernel(State st, PropBuf pb,
                     ov += __shfl_xor_sync(kFull, ov, o);
                 d = ((float)wt[j] - 2.f * (float)ov) / wi;
             }
-            if (lane == 0)
-                x[j] = __float2bfloat16_rn(d);
+            if (lane == 0) {
+                sd[j] = d;
+                sj[j] = (uint16_t)j;
+            }
         }
-        {
-            const uint32_t c = pb.cols[threadIdx.x & 255];
-            const int bit = (int)((ri[c >> 6] >> (c & 63)) & 1ull);
-            x[256 + (threadIdx.x & 255)] = __float2bfloat16_rn(bit ? 1.f : -1.f);
-        }
+        __syncthreads();
+        for (int size = 2; size <= 256; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                const int o = tid ^ stride;
+                if (o > tid) {
+                    const bool up = (tid & size) == 0;
+                    const bool gt = sd[tid] > sd[o] || (sd[tid] == sd[o] && sj[tid] > sj[o]);
+                    if (gt == up) {
+                        const float t0 = sd[tid];
+                        sd[tid] = sd[o];
+                        sd[o] = t0;
+                        const uint16_t u0 = sj[tid];
+                        sj[tid] = sj[o];
+                        sj[o] = u0;
+                    }
+                }
+                __syncthreads();
+            }
+        __nv_bfloat16* x = pb.X + q * 512;
+        const float d = sd[tid];
+        x[tid] = __float2bfloat16_rn(d >= kNoRow ? 4.f : d);
+        pb.perm[q * 256 + tid] = sj[tid];
+        const uint32_t c = pb.cols[tid];
+        x[256 + tid] = __float2bfloat16_rn(((ri[c >> 6] >> (c & 63)) & 1ull) ? 1.f : -1.f);
         __syncthreads();
     }
 }
@@ -117,7 +144,8 @@ __global__ void __launch_bounds__(item::kFwht16Threads)
     search_kernel(State st, PropBuf pb, unsigned long long gen, int cols) {
     extern __shared__ __align__(16) int32_t Psm[];
     __shared__ uint32_t red[16];
-    __shared__ uint16_t win[16];
+    __shared__ uint16_t win[16];   // rows of the window
+    __shared__ uint16_t wpos[16];  // their rank positions
     __shared__ uint64_t s_out_s;
     __shared__ uint32_t s_out_w;
     __shared__ int s_learned;
@@ -139,16 +167,19 @@ __global__ void __launch_bounds__(item::kFwht16Threads)
             if (warp == 0) {
                 const bool learned =
                     pb.mode == 1 && hunit(qhash(pb.seed, gen, q, 0x51)) < pb.learned_frac;
+                // rank positions 0 .. N-2 hold the N-1 rows other than i
                 float sc[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    const int j = lane + 32 * k;
-                    if (j >= N || j == i) {
+                    const int pos = lane + 32 * k;
+                    if (pos >= N - 1) {
                         sc[k] = -INFINITY;
                     } else {
-                        const float u = hunit(qhash(pb.seed, gen, q, 0x1000 + j));
+                        const float u = hunit(qhash(pb.seed, gen, q, 0x1000 + pos));
                         const float gum = -logf(-logf(u));
-                        sc[k] = learned ? pb.logits[q * 256 + j] + gum : gum;
+                        sc[k] = pb.mode == 3 ? -(float)pos  // the 16 best-ranked rows
+                                : learned    ? pb.logits[q * 256 + pos] + gum
+                                             : gum;
                     }
                 }
                 for (int t = 0; t < 16; ++t) {  // Gumbel-top-16: sampling without replacement
@@ -173,8 +204,10 @@ __global__ void __launch_bounds__(item::kFwht16Threads)
                     for (int k = 0; k < 8; ++k)
                         if (lane + 32 * k == bj)
                             sc[k] = -INFINITY;
-                    if (lane == 0)
-                        win[t] = (uint16_t)bj;
+                    if (lane == 0) {
+                        wpos[t] = (uint16_t)bj;
+                        win[t] = pb.perm[q * 256 + bj];
+                    }
                 }
                 if (lane == 0)
                     s_learned = learned ? 1 : 0;
@@ -209,12 +242,12 @@ __global__ void __launch_bounds__(item::kFwht16Threads)
                 if (tid == 0)
                     Wt[i] = wnew;
                 const float share = 1.f / (float)__popc(S);
-                for (int j = tid; j < 256; j += blockDim.x) {
+                for (int pos = tid; pos < 256; pos += blockDim.x) {
                     float v = 0.f;
                     for (int t = 0; t < 16; ++t)
-                        if (win[t] == j && ((S >> t) & 1u))
+                        if (wpos[t] == pos && ((S >> t) & 1u))
                             v = share;
-                    pb.T[q * 256 + j] = v;
+                    pb.T[q * 256 + pos] = v;
                 }
             }
             __syncthreads();
@@ -300,6 +333,8 @@ int propose_setup(bmm_ga* g, int mode, int qpc, int train_steps, float lr, float
     pb.cols = (const uint32_t*)p;
     BMM_TRY(palloc(g, Q * 2, &p));
     pb.target = (uint16_t*)p;
+    BMM_TRY(palloc(g, Q * 256 * 2, &p));
+    pb.perm = (uint16_t*)p;
     BMM_TRY(palloc(g, Q * 512 * 2, &p));
     pb.X = (__nv_bfloat16*)p;
     BMM_TRY(palloc(g, Q * 256 * 4, &p));

@@ -5,8 +5,10 @@
 // mutation partners uniformly (operators.cpp:100-129).
 //
 // Inputs per query (a target row i of an individual): 256 per-row weight
-// features and the ±1 bits of row i's 256-column sketch; outputs: one logit
-// per candidate row j (how likely j belongs to an improving XOR subset for i).
+// features -- the pairwise weight changes of the other rows, in ascending
+// order -- and the ±1 bits of row i's 256-column sketch; outputs: one logit
+// per rank position (how likely the row at that position belongs to an
+// improving XOR subset for i).
 //
 // GEMM kernel.  C[M x N] = A[M x K] . B[N x K]^T for any element strides of A
 // and B (transposes are folded into the staging loads), FP32 or BF16 sources

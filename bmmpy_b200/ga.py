@@ -231,8 +231,9 @@ class ProposalConfig:
 
     mode: "off" (the reference GA), "learned" (windows of 16 rows drawn from
     the proposal network's scores, with uniform exploration, exhaustively
-    searched and trained on the improving subsets) or "uniform" (uniform
-    windows only, the ablation without the network)."""
+    searched and trained on the improving subsets), "uniform" (uniform
+    windows only, the ablation without the network) or "ranked" (the 16
+    rows whose XOR alone changes the target row's weight least)."""
 
     __slots__ = ("mode", "queries_per_elite", "train_steps", "learning_rate",
                  "learned_fraction", "seed")
@@ -240,7 +241,7 @@ class ProposalConfig:
     def __init__(self, mode: str = "off", queries_per_elite: int = 2, train_steps: int = 2,
                  learning_rate: float = 1e-3, learned_fraction: float = 0.5,
                  seed: int = 1) -> None:
-        if mode not in ("off", "learned", "uniform"):
+        if mode not in ("off", "learned", "uniform", "ranked"):
             raise ValueError(f"Unsupported proposal mode: {mode!r}")
         self.mode = mode
         self.queries_per_elite = queries_per_elite
@@ -250,7 +251,7 @@ class ProposalConfig:
         self.seed = seed
 
     def native(self) -> N.GaProposal_t:
-        return N.GaProposal_t({"off": 0, "learned": 1, "uniform": 2}[self.mode],
+        return N.GaProposal_t({"off": 0, "learned": 1, "uniform": 2, "ranked": 3}[self.mode],
                               int(self.queries_per_elite), int(self.train_steps), 0,
                               float(self.learning_rate), float(self.learned_fraction),
                               int(self.seed) & 0xFFFFFFFFFFFFFFFF)
