@@ -11,6 +11,7 @@ does not).
 from __future__ import annotations
 
 from . import ga
+from .apply import ApplyResult, GlobalGreedyApplier, GreedyApplier
 from .candidate import Candidate
 from .ga import (
     GeneticAlgorithm,
@@ -33,7 +34,10 @@ from .search import (
     MitmFwhtSearch,
 )
 
+from .workflows import search_apply
+
 __all__ = [
+    "ApplyResult",
     "BitMatrix",
     "BruteforceSearch",
     "Candidate",
@@ -41,6 +45,8 @@ __all__ = [
     "CudaMitmFwhtSearch",
     "FwhtSearch",
     "GeneticAlgorithm",
+    "GlobalGreedyApplier",
+    "GreedyApplier",
     "IslandModel",
     "IslandModelSnapshot",
     "IslandSnapshot",
@@ -57,4 +63,5 @@ __all__ = [
     "get_runtime_features",
     "get_version",
     "matrix_from_rows",
+    "search_apply",
 ]

@@ -281,6 +281,9 @@ class Ref(_Searches):
         L.refh_ga_run.restype = C.c_long
         L.refh_ga_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, C.POINTER(GaConfig),
                                   C.c_uint64, _sz, _u64p, _u64p, _u32p, C.POINTER(C.c_double)]
+        L.refh_apply.restype = C.c_long
+        L.refh_apply.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _u64p, _sz, _u32p, _sz, C.c_int,
+                                 C.c_uint64, C.c_int, C.c_uint64, C.c_int, _u64p, _u64p, _u64p]
         L.refh_island_run.restype = C.c_long
         L.refh_island_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_uint64,
                                       _sz, C.c_uint64, C.c_double, _u64p, C.POINTER(C.c_double)]
@@ -357,6 +360,28 @@ class Ref(_Searches):
         if g < 0:
             raise ERRORS.get(g, OracleError)("reference error")
         return scores[: g + 1].tolist(), bm, bw, secs.value
+
+    def apply(self, m, cols, win, masks, weights, global_=False, min_gain=1, stochastic=False,
+              seed=0, require_improvement=True):
+        """The reference applier on a copy of m: (new words, applied, improvement).
+        masks: (n_cand, mw) uint64."""
+        win = self._win(win)
+        masks = np.ascontiguousarray(masks, dtype=np.uint64)
+        masks = masks.reshape(len(weights), -1) if len(weights) else np.zeros((0, 1), np.uint64)
+        if masks.shape[1] == 0:
+            masks = np.zeros((len(weights), 1), np.uint64)
+        ws = np.ascontiguousarray(weights, dtype=np.uint32)
+        out = np.zeros_like(m)
+        a = C.c_uint64(0)
+        imp = C.c_uint64(0)
+        rc = self.lib.refh_apply(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], _ptr(win, _szp),
+                                 len(win), _ptr(masks, _u64p), masks.shape[1], _ptr(ws, _u32p),
+                                 len(ws), int(global_), min_gain, int(stochastic), seed,
+                                 int(require_improvement), _ptr(out, _u64p), C.byref(a),
+                                 C.byref(imp))
+        if rc < 0:
+            raise ERRORS.get(rc, OracleError)(f"reference error {rc}")
+        return out, int(a.value), int(imp.value)
 
     def island_run(self, m, cols, win, islands, population, interval, seed, max_gens, target,
                    cap_seconds):

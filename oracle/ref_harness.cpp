@@ -14,6 +14,8 @@
 // a reference exception: -1 std::invalid_argument, -2 std::overflow_error,
 // -3 std::out_of_range, -4 std::logic_error, -5 other std::exception.
 
+#include "bmmpy/apply/global_greedy_applier.hpp"
+#include "bmmpy/apply/greedy_applier.hpp"
 #include "bmmpy/core/bit_matrix.hpp"
 #include "bmmpy/core/row_window.hpp"
 #include "bmmpy/ga/genetic_algorithm.hpp"
@@ -310,6 +312,42 @@ long refh_island_run(const std::uint64_t* words, std::size_t rows, std::size_t c
         model.wait();
         *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         *best_score = model.snapshot().best_score;
+        return 0L;
+    });
+}
+
+// GreedyApplier (stochastic, seed) / GlobalGreedyApplier (require_improvement)
+// applied to the window of the matrix; the matrix words after the apply go to
+// out_words (rows x stride); applied / improvement receive the ApplyResult.
+// Candidate masks: n_cand x mw words.
+long refh_apply(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                std::size_t stride, const std::size_t* win, std::size_t t,
+                const std::uint64_t* cand_masks, std::size_t mw, const std::uint32_t* cand_w,
+                std::size_t n_cand, int global, std::uint64_t min_gain, int stochastic,
+                std::uint64_t seed, int require_improvement, std::uint64_t* out_words,
+                std::uint64_t* applied, std::uint64_t* improvement) {
+    return guarded([&] {
+        auto m = make_matrix(words, rows, cols, stride);
+        auto w = m.row_window(to_rows(win, t));
+        std::vector<bmmpy::Candidate> cands;
+        for (std::size_t c = 0; c < n_cand; ++c) {
+            std::vector<std::uint64_t> mask(cand_masks + c * mw, cand_masks + (c + 1) * mw);
+            cands.emplace_back(std::move(mask), cand_w[c]);
+        }
+        bmmpy::ApplyResult r;
+        if (global) {
+            bmmpy::GlobalGreedyApplier a(require_improvement != 0);
+            r = a.apply(w, cands);
+        } else {
+            bmmpy::GreedyApplier a(min_gain, stochastic != 0, seed);
+            r = a.apply(w, cands);
+        }
+        const std::size_t wpr = m.words_per_row();
+        for (std::size_t i = 0; i < rows; ++i)
+            for (std::size_t q = 0; q < stride; ++q)
+                out_words[i * stride + q] = q < wpr ? m.row_words(i)[q] : 0;
+        *applied = r.applied_count;
+        *improvement = r.weight_improvement;
         return 0L;
     });
 }

@@ -261,3 +261,88 @@ def test_bf16_rounding_is_nearest_even():
     x = np.array([1.0, 1.00390625, 1.01171875, -2.5, 3.0e-3], np.float32)
     # 1 + 2^-8 is a tie -> even (1.0); 1 + 3*2^-8 is a tie -> even (1 + 2^-6)
     assert M.bf16(x).tolist() == [1.0, 1.0, 1.015625, -2.5, np.float32(0.0030059814453125)]
+
+
+def _apply_case(rng, rows, cols, t, n_cand, multiword=False):
+    from bmmpy_b200.candidate import Candidate
+    from bmmpy_b200.matrix import BitMatrix
+
+    P = port()
+    words, _ = P.gen_instance(rows, cols, rng.choice([0.1, 0.3, 0.5]), rng.randint(0, 999),
+                              rng.randint(0, rows))
+    m = BitMatrix(rows, cols)
+    m.words[:] = words[:, : m.stride_words]
+    win = rng.sample(range(rows), t)
+    mw = (t + 63) // 64 if multiword else 1
+    masks = np.zeros((n_cand, mw), np.uint64)
+    weights = np.zeros(n_cand, np.uint32)
+    cands = []
+    for c in range(n_cand):
+        v = rng.getrandbits(t) or 1
+        for q in range(mw):
+            masks[c, q] = np.uint64((v >> (64 * q)) & ((1 << 64) - 1))
+        # weights: the true weight of the combination, sometimes perturbed (stale)
+        acc = np.zeros(m.stride_words, np.uint64)
+        for b in range(t):
+            if (v >> b) & 1:
+                acc ^= m.words[win[b]]
+        wt = int(sum(bin(int(x)).count("1") for x in acc))
+        if rng.random() < 0.2:
+            wt = max(0, wt + rng.randint(-5, 5))
+        weights[c] = wt
+        cands.append(Candidate([int(x) for x in masks[c]], wt))
+    return words, m, win, masks, weights, cands
+
+
+@pytest.mark.skipif(ref() is None, reason="reference library not built (make -C oracle ref)")
+def test_greedy_applier_matches_reference():
+    from bmmpy_b200.apply import GreedyApplier
+
+    R = ref()
+    rng = random.Random(5)
+    for trial in range(60):
+        rows = rng.randint(1, 70)
+        t = rng.randint(1, min(rows, 64))
+        cols = rng.choice([5, 64, 130, 700])
+        words, m, win, masks, weights, cands = _apply_case(rng, rows, cols, t, rng.randint(0, 40))
+        stochastic = rng.random() < 0.4
+        seed = rng.choice([0, 7, 2**63 + 5])
+        min_gain = rng.choice([0, 1, 3])
+        want, a, imp = R.apply(words, cols, win, masks, weights, False, min_gain, stochastic, seed)
+        got = GreedyApplier(min_gain, stochastic=stochastic, seed=seed).apply(
+            m.row_window(win), cands)
+        assert (got.applied_count, got.weight_improvement) == (a, imp)
+        assert np.array_equal(m.words, want[:, : m.stride_words])
+
+
+@pytest.mark.skipif(ref() is None, reason="reference library not built (make -C oracle ref)")
+def test_global_greedy_applier_matches_reference():
+    from bmmpy_b200.apply import GlobalGreedyApplier
+
+    R = ref()
+    rng = random.Random(6)
+    for trial in range(60):
+        rows = rng.randint(1, 90)
+        t = rng.randint(1, min(rows, 80))
+        cols = rng.choice([5, 64, 200])
+        words, m, win, masks, weights, cands = _apply_case(rng, rows, cols, t,
+                                                           rng.randint(0, 30), multiword=True)
+        req = rng.random() < 0.5
+        want, a, imp = R.apply(words, cols, win, masks, weights, True, require_improvement=req)
+        got = GlobalGreedyApplier(require_improvement=req).apply(m.row_window(win), cands)
+        assert (got.applied_count, got.weight_improvement) == (a, imp)
+        assert np.array_equal(m.words, want[:, : m.stride_words])
+
+
+def test_apply_errors_match_reference_classes():
+    from bmmpy_b200.apply import GlobalGreedyApplier, GreedyApplier
+    from bmmpy_b200.candidate import Candidate
+    from bmmpy_b200.matrix import BitMatrix
+
+    m = BitMatrix(70, 8)
+    with pytest.raises(ValueError):
+        GreedyApplier(1).apply(m.row_window(list(range(65))), [])
+    with pytest.raises(RuntimeError):  # mask_u64 of a two-word mask
+        GreedyApplier(1).apply(m.row_window([0, 1]), [Candidate([1, 1], 0)])
+    with pytest.raises(ValueError):  # bits outside the window
+        GlobalGreedyApplier().apply(m.row_window([0, 1]), [Candidate([4], 0)])
