@@ -341,10 +341,11 @@ C3 = dict(rows=512, cols=65536, p=0.02, seed=2, scrambles=2000, window=32)
 
 
 def run_mitm(args):
-    """Search -> apply sweeps over the planted 512 x 65536 matrix: windows of 32
-    consecutive rows (offset by 16 on odd sweeps), each searched exhaustively
-    (all 2^32 subsets, meet-in-the-middle FWHT, top 64) and applied with
-    GreedyApplier(min_gain=1), until a sweep improves nothing or the cap."""
+    """Search -> apply sweeps over the planted 512 x 65536 matrix: every sweep
+    splits the rows into 16 windows of 32 by a seeded random permutation; each
+    window is searched exhaustively (all 2^32 subsets, meet-in-the-middle
+    FWHT, top 64) and applied with GreedyApplier(min_gain=1); until four
+    sweeps in a row improve nothing, or the cap."""
     if args.impl == "reference":
         from oracle.oracle import port, ref
 
@@ -375,15 +376,17 @@ def run_mitm(args):
     applier = bmm.GreedyApplier(1)
     nwin = C3["rows"] // C3["window"]
     sweeps = []
+    rng = np.random.default_rng(C3["seed"])
     t0 = time.perf_counter()
     search_s = 0.0
     windows = 0
     sweep = 0
-    while time.perf_counter() - t0 < args.cap:
-        off = (sweep % 2) * (C3["window"] // 2)
+    idle = 0
+    while time.perf_counter() - t0 < args.cap and idle < 4:
+        perm = rng.permutation(C3["rows"])
         gained = 0
         for j in range(nwin):
-            rows = [(off + C3["window"] * j + r) % C3["rows"] for r in range(C3["window"])]
+            rows = sorted(int(r) for r in perm[C3["window"] * j: C3["window"] * (j + 1)])
             win = m.row_window(rows)
             ts = time.perf_counter()
             cands = searcher.search(win)
@@ -391,10 +394,9 @@ def run_mitm(args):
             windows += 1
             gained += applier.apply(win, cands).weight_improvement
         sweeps.append({"sweep": sweep, "weight": m.weight(), "gained": gained,
-                       "t": time.perf_counter() - t0})
+                       "t": round(time.perf_counter() - t0, 3)})
         sweep += 1
-        if gained == 0:
-            break
+        idle = idle + 1 if gained == 0 else 0
     line = {
         "metric": "recovered weight (search -> apply) vs planted weight",
         "value": m.weight(), "unit": "weight", "higher_is_better": False, "n_gpus": 1,
