@@ -24,6 +24,8 @@
 #include "spectrum.cuh"
 #include "topk.cuh"
 
+#include <algorithm>
+
 namespace bmm {
 namespace {
 
@@ -34,6 +36,17 @@ constexpr int kPer = kTile / kThr;  // 64
 static_assert(kPer == 64, "register rounds assume 64 values per thread");
 
 __device__ __forceinline__ int swz(int k) { return k ^ ((k >> 6) & 31); }
+
+// Middle-pass tile layout: XOR with a multiple of 4 keeps every group of 4
+// consecutive elements contiguous (16-byte copies), and is conflict-free for
+// both register rounds used there (WL = 8: k >> 8 is the same for a warp;
+// WL = 2: the warp's 8 row groups get 8 different XORs).
+__device__ __forceinline__ int swzm(int k) { return k ^ (((k >> 8) & 7) << 2); }
+
+template <bool MID>
+__device__ __forceinline__ int tswz(int k) {
+    return MID ? swzm(k) : swz(k);
+}
 
 // One register round: the thread holds the 64 tile elements
 // k = base(tid) | (e << WL), e in [0, 64), and applies the stages on e bits
@@ -57,29 +70,40 @@ __device__ __forceinline__ void bfly(int32_t (&x)[64]) {
     }
 }
 
-template <int WL, int S0, int NS>
+template <int WL, int S0, int NS, bool MID = false>
 __device__ __forceinline__ void round_load(const int32_t* s, int32_t (&x)[64]) {
     const int base = round_base<WL>(threadIdx.x);
 #pragma unroll
     for (int e = 0; e < 64; ++e)
-        x[e] = s[swz(base | (e << WL))];
+        x[e] = s[tswz<MID>(base | (e << WL))];
     bfly<S0, NS>(x);
 }
 
-template <int WL>
+template <int WL, bool MID = false>
 __device__ __forceinline__ void round_store(int32_t* s, const int32_t (&x)[64]) {
     const int base = round_base<WL>(threadIdx.x);
 #pragma unroll
     for (int e = 0; e < 64; ++e)
-        s[swz(base | (e << WL))] = x[e];
+        s[tswz<MID>(base | (e << WL))] = x[e];
 }
 
 // Offer the 64 register values of the last round to the warp's top-k.
 // Global mask of element k of the tile: mask_of(k).
+// A per-thread minimum over the 64 weights and one warp vote skip the offers
+// whenever no lane can enter the list (the threshold only falls, so the skip
+// is exact); after the first tiles that is nearly always.
 template <int WL, int E, typename MaskOf>
 __device__ __forceinline__ void scan_values(const int32_t (&x)[64], long long N, int kk,
                                             WarpTopK<E>& top, uint32_t& thr, MaskOf mask_of) {
     const int base = round_base<WL>(threadIdx.x);
+    long long lo2 = (long long)UINT32_MAX * 2 + 2;
+#pragma unroll
+    for (int e = 0; e < 64; ++e) {
+        const long long w2 = N - (long long)x[e];
+        lo2 = (w2 >= 0 && (w2 & 1) == 0 && w2 < lo2) ? w2 : lo2;
+    }
+    if (!__any_sync(kFull, (lo2 >> 1) <= (long long)thr))
+        return;
 #pragma unroll
     for (int e = 0; e < 64; ++e) {
         const uint64_t mask = mask_of(base | (e << WL));
@@ -266,7 +290,12 @@ __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
 }
 
 // Middle / last pass over bits [lo, lo + R), R <= 9: tile = 2^R rows
-// (stride 2^lo) x 2^B consecutive elements, B = 14 - R >= 5.
+// (stride 2^lo) x 2^B consecutive elements, B = 14 - R >= 5.  Tiles move
+// from HBM straight into the swizzled shared tile with 4-byte cp.async (a
+// warp copies 32 consecutive elements of one row: full lines), so no register
+// holds a loaded value or its address.  The last pass (one CTA per SM, its
+// scan is the longer phase) double-buffers: tile n+1 is in flight while
+// tile n is transformed and scanned.
 template <int R, bool LAST, int E>
 __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
     pass_mid_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
@@ -285,37 +314,67 @@ __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
         top.init();
         N = (long long)*total;
     }
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const long long lb = tile % lowblocks, hi = tile / lowblocks;
-        const uint64_t gbase = ((uint64_t)hi << (lo + R)) | ((uint64_t)lb << B);
+    auto tile_base = [&](long long tl) -> uint64_t {
+        return ((uint64_t)(tl / lowblocks) << (lo + R)) | ((uint64_t)(tl % lowblocks) << B);
+    };
+    // 16-byte copies: chunk c = 4 consecutive elements k = 4c .. 4c+3 of one row
+    auto issue = [&](long long tl, int32_t* buf) {
+        const uint64_t gb = tile_base(tl);
+        const uint32_t sb = (uint32_t)__cvta_generic_to_shared(buf);
+#pragma unroll 4
+        for (int u = 0; u < kTile / 4 / kThr; ++u) {
+            const int k = (u * kThr + tid) * 4;
+            const uint64_t gi = gb | ((uint64_t)(k >> B) << lo) | (uint64_t)(k & ((1 << B) - 1));
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+                             sb + 4u * (uint32_t)swzm(k)),
+                         "l"(d + gi)
+                         : "memory");
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    long long tile = blockIdx.x;
+    if (LAST && tile < ntiles)
+        issue(tile, s);
+    for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
+        int32_t* cur = LAST ? s + (it & 1) * kTile : s;
+        if (LAST) {
+            const long long nxt = tile + gridDim.x;
+            if (nxt < ntiles) {
+                issue(nxt, s + ((it + 1) & 1) * kTile);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+            } else {
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            }
+        } else {
+            issue(tile, s);
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        }
+        __syncthreads();
+        const uint64_t gbase = tile_base(tile);
         auto gidx = [&](int k) -> uint64_t {
             return gbase | ((uint64_t)(k >> B) << lo) | (uint64_t)(k & ((1 << B) - 1));
         };
-        // round 1 works on k = (e << 8) | tid: load it straight from HBM
-        // (a warp reads 32 consecutive elements of one row: full lines)
         int32_t x[64];
-#pragma unroll
-        for (int e = 0; e < 64; ++e)
-            x[e] = d[gidx((e << 8) | tid)];
         if constexpr (R > 6) {
-            bfly<0, 6>(x);  // k bits 8..13 = the top six stage bits
-            round_store<8>(s, x);
+            round_load<8, 0, 6, true>(cur, x);  // k bits 8..13 = the top six stage bits
+            round_store<8, true>(cur, x);
             __syncthreads();
-            round_load<2, B - 2, R - 6>(s, x);
+            round_load<2, B - 2, R - 6, true>(cur, x);
             if (LAST) {
                 scan_values<2, E>(x, N, kk, top, thr,
                                   [&](int k) { return (xhi << T) | gidx(k); });
             } else {
-                round_store<2>(s, x);
+                round_store<2, true>(cur, x);
                 __syncthreads();
-#pragma unroll
-                for (int e = 0; e < 64; ++e) {
-                    const int k = (e << 8) | tid;
-                    d[gidx(k)] = s[swz(k)];
+#pragma unroll 4
+                for (int u = 0; u < kTile / 4 / kThr; ++u) {
+                    const int k = (u * kThr + tid) * 4;
+                    *reinterpret_cast<int4*>(d + gidx(k)) =
+                        *reinterpret_cast<const int4*>(cur + swzm(k));
                 }
             }
         } else {
-            bfly<B - 8, R>(x);  // stage bits [B, 14) all inside k bits 8..13
+            round_load<8, B - 8, R, true>(cur, x);  // stage bits [B, 14) all inside k bits 8..13
             if (LAST) {
                 scan_values<8, E>(x, N, kk, top, thr,
                                   [&](int k) { return (xhi << T) | gidx(k); });
@@ -396,11 +455,18 @@ constexpr size_t pass_smem(bool last, int E) {
                : kTile * sizeof(int32_t);
 }
 
+// The last middle pass double-buffers its tiles.
+constexpr size_t mid_smem(bool last, int E) {
+    return last ? (pass_smem(true, E) > 2 * kTile * sizeof(int32_t) ? pass_smem(true, E)
+                                                                   : 2 * kTile * sizeof(int32_t))
+                : kTile * sizeof(int32_t);
+}
+
 template <int E>
 int launch_mid(int R, bool last, int32_t* d, int T, int lo, unsigned long long xhi,
                const unsigned long long* total, int kk, bmm_candidate* lists, int grid,
                cudaStream_t st) {
-    const size_t smem = pass_smem(last, E);
+    const size_t smem = mid_smem(last, E);
 #define BMM_MID(RR)                                                                               \
     case RR: {                                                                                    \
         auto k = last ? pass_mid_kernel<RR, true, E> : pass_mid_kernel<RR, false, E>;             \
@@ -498,7 +564,9 @@ int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
     plan_mid(T, widths, &nmid);
     const int grid_a = grid_for(ws, ntiles);
     const int grid_m = grid_for(ws, ntiles);  // every pass has 2^(T-14) tiles
-    const int grid_last = nmid ? grid_m : grid_a;
+    // the double-buffered last middle pass: one persistent CTA per SM
+    const int grid_last =
+        nmid ? (int)std::min<long long>(ntiles, (long long)ws->sm_count) : grid_a;
     const long long slices = 1ll << H;
     bmm_candidate *lists = nullptr, *slice_lists = nullptr;
     BMM_TRY(ws_buffer(ws, kSlotCand, (size_t)grid_last * kk * sizeof(bmm_candidate),
@@ -533,7 +601,8 @@ int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
                 int lo = kTileLog;
                 for (int i = 0; i < nmid; ++i) {
                     BMM_TRY(launch_mid<E>(widths[i], i == nmid - 1, (int32_t*)spec, T, lo,
-                                          (unsigned long long)x, total, kk, lists, grid_m, stream));
+                                          (unsigned long long)x, total, kk, lists,
+                                          i == nmid - 1 ? grid_last : grid_m, stream));
                     lo += widths[i];
                 }
             }

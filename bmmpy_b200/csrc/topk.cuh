@@ -18,6 +18,7 @@ template <int E>
 struct WarpTopK {
     uint32_t w[E];
     uint64_t m[E];
+    uint64_t thr_m;  // mask of entry kk-1 (warp-uniform), with the caller's weight `thr`
 
     __device__ __forceinline__ void init() {
 #pragma unroll
@@ -25,6 +26,20 @@ struct WarpTopK {
             w[e] = 0xffffffffu;
             m[e] = ~0ull;
         }
+        thr_m = ~0ull;
+    }
+
+    // mask of entry kk-1
+    __device__ __forceinline__ uint64_t threshold_mask(int kk) const {
+        const int idx = kk - 1;
+        const int src_lane = idx / E;
+        const int src_e = idx % E;
+        uint64_t mine = m[0];
+#pragma unroll
+        for (int e = 1; e < E; ++e)
+            if (e == src_e)
+                mine = m[e];
+        return __shfl_sync(kFull, mine, src_lane);
     }
 
     // weight of entry kk-1 (the pruning threshold for a top-kk request)
@@ -67,18 +82,22 @@ struct WarpTopK {
     }
 
     // Offer one candidate per lane (ok == false lanes offer nothing).
-    // `thr` caches threshold(kk) and is refreshed after every insertion.
+    // `thr` caches threshold(kk) (and thr_m its mask); both are refreshed
+    // after every insertion.  Only offers ordered before entry kk-1 pass the
+    // ballot, so ties at the threshold weight with a larger mask -- common in
+    // large spectra -- never reach the insertion.
     __device__ __forceinline__ void offer(bool ok, uint32_t wv, uint64_t mv, int kk,
                                          uint32_t& thr) {
-        unsigned bal = __ballot_sync(kFull, ok && wv <= thr);
+        unsigned bal = __ballot_sync(kFull, ok && (wv < thr || (wv == thr && mv < thr_m)));
         while (bal) {
             const int src = __ffs(bal) - 1;
             const uint32_t wi = __shfl_sync(kFull, wv, src);
             const uint64_t mi = __shfl_sync(kFull, mv, src);
             insert(wi, mi);
             thr = threshold(kk);
+            thr_m = threshold_mask(kk);
             bal &= ~(1u << src);
-            bal &= __ballot_sync(kFull, ok && wv <= thr);
+            bal &= __ballot_sync(kFull, ok && (wv < thr || (wv == thr && mv < thr_m)));
         }
     }
 
