@@ -96,14 +96,26 @@ template <int WL, int E, typename MaskOf>
 __device__ __forceinline__ void scan_values(const int32_t (&x)[64], long long N, int kk,
                                             WarpTopK<E>& top, uint32_t& thr, MaskOf mask_of) {
     const int base = round_base<WL>(threadIdx.x);
-    long long lo2 = (long long)UINT32_MAX * 2 + 2;
+    if (N < (1ll << 30)) {  // |x| <= N: 2*weight = N - x fits 32 bits
+        const uint32_t n32 = (uint32_t)N;
+        uint32_t lo2 = 0xffffffffu;
 #pragma unroll
-    for (int e = 0; e < 64; ++e) {
-        const long long w2 = N - (long long)x[e];
-        lo2 = (w2 >= 0 && (w2 & 1) == 0 && w2 < lo2) ? w2 : lo2;
+        for (int e = 0; e < 64; ++e) {
+            const uint32_t w2 = n32 - (uint32_t)x[e];
+            lo2 = (w2 & 1u) ? lo2 : min(lo2, w2);
+        }
+        if (!__any_sync(kFull, lo2 != 0xffffffffu && (lo2 >> 1) <= thr))
+            return;
+    } else {
+        long long lo2 = (long long)UINT32_MAX * 2 + 2;
+#pragma unroll
+        for (int e = 0; e < 64; ++e) {
+            const long long w2 = N - (long long)x[e];
+            lo2 = (w2 >= 0 && (w2 & 1) == 0 && w2 < lo2) ? w2 : lo2;
+        }
+        if (!__any_sync(kFull, (lo2 >> 1) <= (long long)thr))
+            return;
     }
-    if (!__any_sync(kFull, (lo2 >> 1) <= (long long)thr))
-        return;
 #pragma unroll
     for (int e = 0; e < 64; ++e) {
         const uint64_t mask = mask_of(base | (e << WL));
