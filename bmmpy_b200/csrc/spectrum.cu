@@ -186,34 +186,55 @@ __global__ void tile_count_kernel(const uint64_t* __restrict__ pats,
 }
 
 // Exclusive scan of n counts (one CTA of 1024 threads); offsets has n + 1
-// entries; cursor receives a copy of the first n offsets.
+// entries; cursor receives a copy of the first n offsets.  Coalesced chunks of
+// 1024 counts: warp-shuffle scans, one shared step, a running total.
 __global__ void __launch_bounds__(1024) exclusive_scan_kernel(const unsigned* __restrict__ counts,
                                                               long long n,
                                                               unsigned* __restrict__ offsets,
                                                               unsigned* __restrict__ cursor) {
-    __shared__ unsigned sums[1024];
-    const long long per = (n + 1023) / 1024;
-    const long long lo = threadIdx.x * per;
-    const long long hi = lo + per < n ? lo + per : n;
-    unsigned s = 0;
-    for (long long i = lo; i < hi; ++i)
-        s += counts[i];
-    sums[threadIdx.x] = s;
+    __shared__ unsigned wsum[32];
+    __shared__ unsigned s_run;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0)
+        s_run = 0;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
-        const unsigned v = threadIdx.x >= (unsigned)off ? sums[threadIdx.x - off] : 0u;
+    for (long long c0 = 0; c0 < n; c0 += 1024) {
+        const long long i = c0 + tid;
+        const unsigned v = i < n ? counts[i] : 0u;
+        unsigned incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o)
+                incl += t;
+        }
+        if (lane == 31)
+            wsum[warp] = incl;
         __syncthreads();
-        sums[threadIdx.x] += v;
+        if (warp == 0) {
+            unsigned ws = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned t = __shfl_up_sync(kFull, ws, o);
+                if (lane >= o)
+                    ws += t;
+            }
+            wsum[lane] = ws;  // inclusive over warps
+        }
+        __syncthreads();
+        const unsigned run = s_run;
+        const unsigned excl = run + (warp ? wsum[warp - 1] : 0u) + incl - v;
+        if (i < n) {
+            offsets[i] = excl;
+            cursor[i] = excl;
+        }
+        __syncthreads();
+        if (tid == 0)
+            s_run = run + wsum[31];
         __syncthreads();
     }
-    unsigned run = threadIdx.x ? sums[threadIdx.x - 1] : 0u;
-    for (long long i = lo; i < hi; ++i) {
-        offsets[i] = run;
-        cursor[i] = run;
-        run += counts[i];
-    }
-    if (threadIdx.x == 1023)
-        offsets[n] = sums[1023];
+    if (tid == 0)
+        offsets[n] = s_run;
 }
 
 __global__ void tile_scatter_kernel(const uint64_t* __restrict__ pats,
