@@ -12,7 +12,6 @@
  *                        CudaBruteforceSearch::search src/search/cuda_bruteforce_search.cpp:38-103
  *                        run_cuda_bruteforce_search  include/bmmpy/search/cuda_bruteforce_launch.hpp:22-23
  *   bmm_fwht_i32/_i16    fwht_inplace                include/bmmpy/math/fwht.hpp:8-9
- *   bmm_split_window     build_compact_split_window  include/bmmpy/search/split_window_prep.hpp:21-26
  *   bmm_runtime_features get_runtime_features        include/bmmpy/stub.hpp:19-21
  *   bmm_gray_targets / bmm_fwht_targets / bmm_batch_fwht_targets
  *                        per-target form of the searches above: for target
