@@ -10,7 +10,7 @@ does not).
 
 from __future__ import annotations
 
-from . import ga
+from . import ga, solver
 from .apply import ApplyResult, GlobalGreedyApplier, GreedyApplier
 from .candidate import Candidate
 from .ga import (
@@ -24,7 +24,7 @@ from .ga import (
     RunStats,
     StopCriteria,
 )
-from .matrix import BitMatrix, RowWindow, matrix_from_rows
+from .matrix import BitMatrix, MatrixError, RowWindow, matrix_from_rows
 from .runtime import RuntimeFeatures, fwht_i16, fwht_i32, get_runtime_features, get_version
 from .search import (
     BruteforceSearch,
@@ -62,6 +62,8 @@ __all__ = [
     "fwht_i32",
     "get_runtime_features",
     "get_version",
+    "MatrixError",
     "matrix_from_rows",
+    "solver",
     "search_apply",
 ]

@@ -16,7 +16,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbmm_b200.so")
 
-OK, EINVAL, EOVERFLOW, ECUDA, ENODEV, ETIMEOUT, ENOMEM = 0, -1, -2, -3, -4, -5, -6
+OK, EINVAL, EOVERFLOW, ECUDA, ENODEV, ETIMEOUT, ENOMEM, ERUNTIME = 0, -1, -2, -3, -4, -5, -6, -7
 
 
 class Candidate_t(C.Structure):
@@ -98,6 +98,20 @@ class GaStats_t(C.Structure):
                 ("best_score", C.c_uint64), ("done", C.c_uint32),
                 ("no_improvement", C.c_uint32), ("mutation_rate", C.c_double)]
 
+class ExactBasisConfig_t(C.Structure):
+    """bmm_exact_basis_config (ExactBasisSolverConfig)."""
+
+    _fields_ = [("max_rows", C.c_size_t), ("max_states", C.c_uint64),
+                ("max_storage_bytes", C.c_size_t)]
+
+
+class ExactBasisResult_t(C.Structure):
+    """bmm_exact_basis_result (ExactBasisResult without its matrices)."""
+
+    _fields_ = [("input_rows", C.c_size_t), ("cols", C.c_size_t), ("rank", C.c_size_t),
+                ("enumerated_states", C.c_uint64), ("total_weight", C.c_uint64)]
+
+
 # name -> argtypes (all return int unless listed in _RESTYPES)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
@@ -145,6 +159,9 @@ SIGNATURES = {
     "bmm_mlp_grads": [_vp, _f32p, _f32p, _sz, _f32p, _f32p],
     "bmm_mlp_train": [_vp, _f32p, _f32p, _sz, C.c_int, _f32p],
     "bmm_mlp_gemm": [_f32p, _f32p, C.c_int, C.c_int, C.c_int, _f32p],
+    "bmm_exact_basis": [_u64p, _sz, _sz, _u32p, _sz, C.POINTER(ExactBasisConfig_t),
+                        C.POINTER(ExactBasisResult_t), _u32p, _u32p],
+    "bmm_basis_weight_counts": [_u64p, _sz, _sz, _u32p, _sz, _u64p],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
              "bmm_gen_instance": C.c_uint64, "bmm_mlp_param_count": C.c_size_t}

@@ -30,6 +30,37 @@ def _popcount_words(a: np.ndarray) -> int:
     return int(np.unpackbits(np.ascontiguousarray(a).view(np.uint8)).sum())
 
 
+class MatrixError(RuntimeError):
+    """bmmpy.MatrixError (include/bmmpy/core/bit_matrix.hpp:14, src/core/bit_matrix.cpp:10-20)."""
+
+
+def _dimension_mismatch() -> MatrixError:
+    return MatrixError("Matrix dimensions mismatch")
+
+
+def gf2_rank_words(words: np.ndarray, cols: int) -> int:
+    """Rank over GF(2) of packed rows (src/core/bit_matrix_algebra.cpp:76-99)."""
+    a = np.array(words, dtype=np.uint64, copy=True)
+    rows = a.shape[0]
+    rank = 0
+    for c in range(cols):
+        if rank == rows:
+            break
+        w, b = divmod(c, WORD_BITS)
+        bit = np.uint64(1 << b)
+        hits = np.nonzero(a[rank:, w] & bit)[0]
+        if hits.size == 0:
+            continue
+        piv = rank + int(hits[0])
+        if piv != rank:
+            a[[rank, piv]] = a[[piv, rank]]
+        below = rank + 1 + np.nonzero(a[rank + 1:, w] & bit)[0]
+        if below.size:
+            a[below] ^= a[rank]
+        rank += 1
+    return rank
+
+
 class BitMatrix:
     __slots__ = ("_rows", "_cols", "_words")
 
@@ -142,6 +173,42 @@ class BitMatrix:
 
     def swap_rows(self, r1: int, r2: int) -> None:
         self._words[[r1, r2]] = self._words[[r2, r1]]
+
+    # -- GF(2) algebra (src/core/bit_matrix_algebra.cpp) -----------------------
+    @classmethod
+    def identity(cls, n: int) -> "BitMatrix":
+        m = cls(n, n)
+        for i in range(n):
+            m.set(i, i, True)
+        return m
+
+    def rank(self) -> int:
+        return gf2_rank_words(self._words, self._cols)
+
+    def add(self, other: "BitMatrix") -> "BitMatrix":
+        if self.shape != other.shape:
+            raise _dimension_mismatch()
+        m = self.copy()
+        m._words ^= other._words
+        return m
+
+    def mul(self, other: "BitMatrix") -> "BitMatrix":
+        """Product over GF(2): row i of the result XORs the rows k of ``other``
+        with bit k set in row i of ``self``."""
+        if self._cols != other.rows:
+            raise _dimension_mismatch()
+        m = BitMatrix(self._rows, other.cols)
+        if self._rows == 0 or self._cols == 0:
+            return m
+        bits = np.unpackbits(self._words.view(np.uint8).reshape(self._rows, -1), axis=1,
+                             bitorder="little")[:, : self._cols]
+        for i in range(self._rows):
+            ks = np.nonzero(bits[i])[0]
+            if ks.size:
+                m._words[i] = np.bitwise_xor.reduce(other._words[ks], axis=0)
+        return m
+
+    __matmul__ = mul
 
     def row_window(self, rows: Sequence[int]) -> "RowWindow":
         return RowWindow(self, rows)

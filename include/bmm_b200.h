@@ -24,13 +24,16 @@
  *                        src/ga/genetic_algorithm_operators.cpp:15-192,
  *                        src/ga/genetic_algorithm_internal.hpp:41-103,
  *                        src/ga/island.cpp:149-228.
+ *   bmm_exact_basis      ExactBasisSolver::solve
+ *                        src/solver/exact_basis_solver.cpp:58-157,
+ *                        include/bmmpy/solver/exact_basis_solver.hpp:12-43.
  *
  * Conventions
  *  - Every function returns an int status (BMM_OK == 0, negative on error)
  *    and never throws; bmm_last_error() gives the calling thread's message.
  *    The status classes map to the reference's exception types:
  *    BMM_EINVAL -> std::invalid_argument, BMM_EOVERFLOW -> std::overflow_error,
- *    BMM_ECUDA / BMM_ENODEV / BMM_ETIMEOUT -> std::runtime_error.
+ *    BMM_ECUDA / BMM_ENODEV / BMM_ETIMEOUT / BMM_ERUNTIME -> std::runtime_error.
  *  - A matrix is row-major packed uint64 words: bit c of a row sits in word
  *    c >> 6 at bit c & 63; `stride` words separate rows; bits at and past
  *    `cols` must be zero (the reference BitMatrix layout).  A window is a list
@@ -68,6 +71,7 @@ extern "C" {
 #define BMM_ENODEV (-4)
 #define BMM_ETIMEOUT (-5)
 #define BMM_ENOMEM (-6)
+#define BMM_ERUNTIME (-7)
 
 /* DeviceTopKEntry of include/bmmpy/search/cuda_launch_topk.cuh:11-14 (16 B). */
 typedef struct bmm_candidate {
@@ -368,6 +372,42 @@ BMM_API int bmm_mlp_train(bmm_mlp* h, const float* x, const float* target, size_
                           int steps, float* loss);
 /* C[M][N] = bf16(A[M][K]) . bf16(B[N][K])^T in FP32 on the tensor cores */
 BMM_API int bmm_mlp_gemm(const float* A, const float* B, int M, int N, int K, float* C);
+
+/* ---- exact minimum-weight basis of a window ------------------------------
+ * ExactBasisSolverConfig / ExactBasisResult of
+ * include/bmmpy/solver/exact_basis_solver.hpp:12-29 (the two matrices are
+ * left to the caller: transform row k = basis_masks[k] over the t window rows,
+ * basis row k = that combination of the rows). */
+typedef struct bmm_exact_basis_config {
+    size_t max_rows;          /* reference default 24 */
+    uint64_t max_states;      /* reference default 2^24 - 1 */
+    size_t max_storage_bytes; /* reference default 128 MiB */
+} bmm_exact_basis_config;
+
+typedef struct bmm_exact_basis_result {
+    size_t input_rows;
+    size_t cols;
+    size_t rank;
+    uint64_t enumerated_states;
+    uint64_t total_weight;
+} bmm_exact_basis_result;
+
+/* ExactBasisSolver::solve (src/solver/exact_basis_solver.cpp:58-157): among
+ * all bases of the window's row space, the one the reference's greedy picks
+ * over the 2^t - 1 combinations ordered by (weight, Gray enumeration index).
+ * basis_masks / basis_weights receive `rank` entries (room for min(t, cols)),
+ * in acceptance order.  Errors: the reference's messages, BMM_EINVAL for its
+ * std::invalid_argument checks, BMM_ERUNTIME for its std::runtime_error. */
+BMM_API int bmm_exact_basis(const uint64_t* words, size_t stride, size_t cols,
+                            const uint32_t* win, size_t t, const bmm_exact_basis_config* cfg,
+                            bmm_exact_basis_result* res, uint32_t* basis_masks,
+                            uint32_t* basis_weights);
+
+/* Weight histogram of the 2^t - 1 nonzero combinations of a window (t <= 32):
+ * counts[w] for w in [0, cols] (the counting pass of
+ * src/solver/exact_basis_solver.cpp:107-118). */
+BMM_API int bmm_basis_weight_counts(const uint64_t* words, size_t stride, size_t cols,
+                                    const uint32_t* win, size_t t, uint64_t* counts);
 
 #ifdef __cplusplus
 }

@@ -953,3 +953,135 @@ long orc_ga_run(const uint64_t* words, size_t stride, size_t cols, const size_t*
     free(pm);
     return steps;
 }
+
+/* ---- ExactBasisSolver (src/solver/exact_basis_solver.cpp:29-157) ---------- */
+static void window_rows(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                        size_t t, uint64_t* rows) {
+    const size_t W = (cols + 63) / 64;
+    const uint64_t tail = tail_mask_for_cols(cols);
+    for (size_t r = 0; r < t; ++r)
+        for (size_t w = 0; w < W; ++w)
+            rows[r * W + w] = words[win[r] * stride + w] & (w + 1 == W ? tail : ~0ull);
+}
+
+static uint32_t combo_weight(const uint64_t* cur, size_t W) {
+    uint32_t s = 0;
+    for (size_t w = 0; w < W; ++w)
+        s += popc64(cur[w]);
+    return s;
+}
+
+int orc_basis_weight_counts(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                            size_t t, uint64_t* counts) {
+    const size_t W = (cols + 63) / 64;
+    memset(counts, 0, (cols + 1) * sizeof(uint64_t));
+    if (t == 0)
+        return 0;
+    if (t > 32)
+        return -1;
+    uint64_t* rows = (uint64_t*)calloc(t * W + 1, sizeof(uint64_t));
+    uint64_t* cur = (uint64_t*)calloc(W + 1, sizeof(uint64_t));
+    if (!rows || !cur) {
+        free(rows);
+        free(cur);
+        return -2;
+    }
+    window_rows(words, stride, cols, win, t, rows);
+    const uint64_t states = (1ull << t) - 1;
+    uint32_t prev = 0;
+    for (uint64_t index = 1; index <= states; ++index) {
+        const uint32_t gray = (uint32_t)(index ^ (index >> 1));
+        const size_t r = ctz64((uint64_t)(gray ^ prev));
+        for (size_t w = 0; w < W; ++w)
+            cur[w] ^= rows[r * W + w];
+        ++counts[combo_weight(cur, W)];
+        prev = gray;
+    }
+    free(rows);
+    free(cur);
+    return 0;
+}
+
+long orc_exact_basis(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                     size_t t, uint32_t* masks, uint32_t* weights, uint64_t* total) {
+    *total = 0;
+    if (t == 0)
+        return 0;
+    if (t > 32)
+        return -1;
+    const size_t W = (cols + 63) / 64, mw = W ? W : 1;
+    const uint64_t states = (1ull << t) - 1;
+    uint64_t* rows = (uint64_t*)calloc(t * mw, sizeof(uint64_t));
+    uint64_t* cur = (uint64_t*)calloc(mw, sizeof(uint64_t));
+    uint64_t* tmp = (uint64_t*)calloc(mw, sizeof(uint64_t));
+    uint64_t* basis = (uint64_t*)calloc((cols + 1) * mw, sizeof(uint64_t));
+    unsigned char* used = (unsigned char*)calloc(cols + 1, 1);
+    uint64_t* offs = (uint64_t*)calloc(cols + 2, sizeof(uint64_t));
+    uint32_t* packed = (uint32_t*)malloc((size_t)states * sizeof(uint32_t));
+    long rc = -2;
+    if (!rows || !cur || !tmp || !basis || !used || !offs || !packed)
+        goto done;
+    window_rows(words, stride, cols, win, t, rows);
+    /* rank of the materialized window */
+    size_t rank = 0;
+    for (size_t r = 0; r < t; ++r)
+        rank += (size_t)pivot_try_insert(basis, used, rows + r * mw, mw, tmp);
+    memset(basis, 0, (cols + 1) * mw * sizeof(uint64_t));
+    memset(used, 0, cols + 1);
+    if (rank == 0) {
+        rc = 0;
+        goto done;
+    }
+    /* counting sort of the Gray enumeration by weight */
+    for (int pass = 0; pass < 2; ++pass) {
+        uint32_t prev = 0;
+        memset(cur, 0, mw * sizeof(uint64_t));
+        for (uint64_t index = 1; index <= states; ++index) {
+            const uint32_t gray = (uint32_t)(index ^ (index >> 1));
+            const size_t r = ctz64((uint64_t)(gray ^ prev));
+            for (size_t w = 0; w < mw; ++w)
+                cur[w] ^= rows[r * mw + w];
+            const uint32_t wt = combo_weight(cur, mw);
+            if (pass == 0)
+                ++offs[wt + 1];
+            else
+                packed[offs[wt]++] = gray;
+            prev = gray;
+        }
+        if (pass == 0)
+            for (size_t w = 0; w <= cols; ++w)
+                offs[w + 1] += offs[w];
+        else
+            for (size_t w = cols + 1; w-- > 0;)
+                offs[w + 1] = offs[w]; /* restore bucket starts */
+        if (pass == 1)
+            offs[0] = 0;
+    }
+    /* greedy insertion, lightest bucket first */
+    size_t got = 0;
+    for (size_t wt = 0; wt <= cols && got < rank; ++wt)
+        for (uint64_t i = offs[wt]; i < offs[wt + 1] && got < rank; ++i) {
+            const uint32_t mask = packed[i];
+            memset(cur, 0, mw * sizeof(uint64_t));
+            for (size_t r = 0; r < t; ++r)
+                if ((mask >> r) & 1u)
+                    for (size_t w = 0; w < mw; ++w)
+                        cur[w] ^= rows[r * mw + w];
+            if (!pivot_try_insert(basis, used, cur, mw, tmp))
+                continue;
+            masks[got] = mask;
+            weights[got] = (uint32_t)wt;
+            *total += wt;
+            ++got;
+        }
+    rc = (long)got;
+done:
+    free(rows);
+    free(cur);
+    free(tmp);
+    free(basis);
+    free(used);
+    free(offs);
+    free(packed);
+    return rc;
+}

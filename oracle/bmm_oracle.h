@@ -123,6 +123,19 @@ long orc_ga_run(const uint64_t* words, size_t stride, size_t cols, const size_t*
                 const orc_ga_config* cfg, uint64_t seed, uint64_t max_steps, uint64_t* scores,
                 uint64_t* best_masks, uint32_t* best_weights);
 
+/* ExactBasisSolver::solve (src/solver/exact_basis_solver.cpp:58-157) without
+ * its configurable caps: every nonzero combination of the t <= 32 window rows
+ * in reflected-Gray order, bucketed by weight, offered in that order to a
+ * greedy GF(2) basis until the window's rank is reached.  masks / weights get
+ * the accepted combinations (room for t); *total their total weight.
+ * Returns the rank, -1 when t > 32, -2 when memory runs out. */
+long orc_exact_basis(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                     size_t t, uint32_t* masks, uint32_t* weights, uint64_t* total);
+
+/* Weight histogram of the 2^t - 1 nonzero combinations (counts[0..cols]). */
+int orc_basis_weight_counts(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
+                            size_t t, uint64_t* counts);
+
 #ifdef __cplusplus
 }
 #endif

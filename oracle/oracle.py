@@ -22,6 +22,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libbmmref.so")
+# the reference built without its AVX2 backend (used for ExactBasisSolver,
+# which the AVX2 build crashes on for rows of 4+ words: aligned loads in
+# src/core/bit_ops_avx2.cpp:21-24 on an unaligned std::vector)
+REF_SCALAR_SO = os.path.join(HERE, "_ref", "libbmmref_scalar.so")
 
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
@@ -100,6 +104,9 @@ def _load_port():
     lib.orc_ga_run.restype = C.c_long
     lib.orc_ga_run.argtypes = [_u64p, _sz, _sz, _szp, _sz, C.POINTER(GaConfig), C.c_uint64,
                                C.c_uint64, _u64p, _u64p, _u32p]
+    lib.orc_exact_basis.restype = C.c_long
+    lib.orc_exact_basis.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u32p, _u32p, _u64p]
+    lib.orc_basis_weight_counts.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p]
     return lib
 
 
@@ -240,6 +247,28 @@ class Port(_Searches):
                                _ptr(cw, _u32p))
         return cm, cw
 
+    def exact_basis(self, m, cols, win):
+        """ExactBasisSolver without caps: (masks, weights, total_weight)."""
+        win = self._win(win)
+        t = len(win)
+        masks = np.zeros(max(t, 1), np.uint32)
+        ws = np.zeros(max(t, 1), np.uint32)
+        total = C.c_uint64(0)
+        r = self.lib.orc_exact_basis(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp), t,
+                                     _ptr(masks, _u32p), _ptr(ws, _u32p), C.byref(total))
+        if r < 0:
+            raise ERRORS.get(r, OracleError)(f"oracle error {r}")
+        return [int(x) for x in masks[:r]], [int(x) for x in ws[:r]], int(total.value)
+
+    def basis_weight_counts(self, m, cols, win):
+        win = self._win(win)
+        counts = np.zeros(cols + 1, np.uint64)
+        rc = self.lib.orc_basis_weight_counts(_ptr(m, _u64p), m.shape[1], cols, _ptr(win, _szp),
+                                              len(win), _ptr(counts, _u64p))
+        if rc < 0:
+            raise ERRORS.get(rc, OracleError)(f"oracle error {rc}")
+        return counts
+
     def ga_run(self, m, cols, win, cfg: GaConfig, seed, max_steps):
         """initialize() + step()s: (scores per step, best masks (n, mw), best weights)."""
         win = self._win(win)
@@ -284,6 +313,9 @@ class Ref(_Searches):
         L.refh_apply.restype = C.c_long
         L.refh_apply.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _u64p, _sz, _u32p, _sz, C.c_int,
                                  C.c_uint64, C.c_int, C.c_uint64, C.c_int, _u64p, _u64p, _u64p]
+        L.refh_exact_basis.restype = C.c_long
+        L.refh_exact_basis.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, C.c_uint64, _sz,
+                                       _u64p, _u32p, _u32p, _u64p, _u64p]
         L.refh_island_run.restype = C.c_long
         L.refh_island_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_uint64,
                                       _sz, C.c_uint64, C.c_double, _u64p, C.POINTER(C.c_double)]
@@ -383,6 +415,29 @@ class Ref(_Searches):
             raise ERRORS.get(rc, OracleError)(f"reference error {rc}")
         return out, int(a.value), int(imp.value)
 
+    def exact_basis(self, m, cols, win, max_rows=24, max_states=(1 << 24) - 1,
+                    max_storage_bytes=128 * 1024 * 1024):
+        """The reference ExactBasisSolver: dict of the ExactBasisResult fields
+        (transform rows as ints, basis_matrix as (rank, stride) words)."""
+        win = self._win(win)
+        t = len(win)
+        sc = np.zeros(5, np.uint64)
+        masks = np.zeros(max(t, 1), np.uint32)
+        ws = np.zeros(max(t, 1), np.uint32)
+        tr = np.zeros(max(t, 1), np.uint64)
+        bw = np.zeros((max(t, 1), m.shape[1]), np.uint64)
+        r = self.lib.refh_exact_basis(_ptr(m, _u64p), m.shape[0], cols, m.shape[1],
+                                      _ptr(win, _szp), t, max_rows, max_states, max_storage_bytes,
+                                      _ptr(sc, _u64p), _ptr(masks, _u32p), _ptr(ws, _u32p),
+                                      _ptr(tr, _u64p), _ptr(bw, _u64p))
+        if r < 0:
+            raise ERRORS.get(r, OracleError)(f"reference error {r}")
+        return {"input_rows": int(sc[0]), "cols": int(sc[1]), "rank": int(sc[2]),
+                "enumerated_states": int(sc[3]), "total_weight": int(sc[4]),
+                "basis_masks": [int(x) for x in masks[:r]],
+                "basis_weights": [int(x) for x in ws[:r]],
+                "transform": [int(x) for x in tr[:r]], "basis_words": bw[:r].copy()}
+
     def island_run(self, m, cols, win, islands, population, interval, seed, max_gens, target,
                    cap_seconds):
         win = self._win(win)
@@ -416,3 +471,14 @@ def ref():
     if _ref is None and os.path.exists(REF_SO):
         _ref = Ref(C.CDLL(REF_SO))
     return _ref
+
+
+_ref_scalar = None
+
+
+def ref_scalar():
+    """The reference built without its AVX2 backend, or None."""
+    global _ref_scalar
+    if _ref_scalar is None and os.path.exists(REF_SCALAR_SO):
+        _ref_scalar = Ref(C.CDLL(REF_SCALAR_SO))
+    return _ref_scalar

@@ -26,6 +26,7 @@
 #include "bmmpy/search/fwht_search.hpp"
 #include "bmmpy/search/mitm_fwht_search.hpp"
 #include "bmmpy/search/split_window_prep.hpp"
+#include "bmmpy/solver/exact_basis_solver.hpp"
 
 #include <chrono>
 #include <cstdint>
@@ -349,6 +350,43 @@ long refh_apply(const std::uint64_t* words, std::size_t rows, std::size_t cols,
         *applied = r.applied_count;
         *improvement = r.weight_improvement;
         return 0L;
+    });
+}
+
+// ExactBasisSolver({max_rows, max_states, max_storage_bytes}).solve(window).
+// scalars[0..4] = input_rows, cols, rank, enumerated_states, total_weight;
+// masks / weights get basis_masks / basis_weights (room for t); transform
+// receives rank words (row k of transform_matrix, t <= 64 columns) and
+// basis_words rank x stride words of basis_matrix.  Returns the rank.
+long refh_exact_basis(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                      std::size_t stride, const std::size_t* win, std::size_t t,
+                      std::size_t max_rows, std::uint64_t max_states, std::size_t max_storage,
+                      std::uint64_t* scalars, std::uint32_t* masks, std::uint32_t* weights,
+                      std::uint64_t* transform, std::uint64_t* basis_words) {
+    return guarded([&] {
+        auto m = make_matrix(words, rows, cols, stride);
+        auto w = m.row_window(to_rows(win, t));
+        bmmpy::ExactBasisSolverConfig cfg;
+        cfg.max_rows = max_rows;
+        cfg.max_states = max_states;
+        cfg.max_storage_bytes = max_storage;
+        const bmmpy::ExactBasisResult r = bmmpy::ExactBasisSolver(cfg).solve(w);
+        scalars[0] = r.input_rows;
+        scalars[1] = r.cols;
+        scalars[2] = r.rank;
+        scalars[3] = r.enumerated_states;
+        scalars[4] = r.total_weight;
+        for (std::size_t k = 0; k < r.basis_masks.size(); ++k) {
+            masks[k] = r.basis_masks[k];
+            weights[k] = r.basis_weights[k];
+        }
+        for (std::size_t k = 0; k < r.transform_matrix.rows(); ++k)
+            transform[k] = r.transform_matrix.cols() ? r.transform_matrix.row_words(k)[0] : 0;
+        const std::size_t wpr = r.basis_matrix.words_per_row();
+        for (std::size_t k = 0; k < r.basis_matrix.rows(); ++k)
+            for (std::size_t q = 0; q < stride; ++q)
+                basis_words[k * stride + q] = q < wpr ? r.basis_matrix.row_words(k)[q] : 0;
+        return static_cast<long>(r.rank);
     });
 }
 

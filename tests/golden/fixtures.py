@@ -43,6 +43,17 @@ GA_CASES = [
      dict(population_size=12, max_generations=4), 4, 77),
 ]
 
+# ExactBasisSolver windows pinned by the reference:
+# (rows, cols, p, instance seed, scrambles, window rows)
+BASIS_CASES = [
+    (24, 256, 0.5, 11, 0, list(range(24))),           # the default max_rows cap
+    (20, 96, 0.08, 12, 40, list(range(19, -1, -1))),   # sparse, planted, reversed window
+    (18, 12, 0.4, 14, 0, list(range(18))),            # rank 12 < rows
+    (30, 2000, 0.02, 15, 60, list(range(3, 19))),      # wide sparse rows, 16-row window
+    (14, 140000, 0.01, 16, 20, list(range(14))),       # rows wider than one shared-memory slab
+    (9, 64, 0.3, 17, 0, [8, 0, 7, 1, 6, 2, 5, 3, 4]),
+]
+
 
 def stride_for(cols: int) -> int:
     words = (cols + 63) // 64

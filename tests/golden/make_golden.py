@@ -17,7 +17,11 @@ library (oracle/_ref/libbmmref.so), called through oracle/ref_harness.cpp:
   C4 batch as per-instance checksums) and MITM top-k lists for windows of the
   C3 planted instance, and single-island GeneticAlgorithm trajectories (best
   score after every step, final best individual) for the GA_CASES of
-  fixtures.py.  Matrices are regenerated from their seeds at test time
+  fixtures.py, and ExactBasisSolver results (basis masks and weights, total
+  weight, rank, transform rows, basis matrix words up to 4096 columns) for
+  the BASIS_CASES windows (from oracle/_ref/libbmmref_scalar.so, the
+  reference built without its AVX2 backend, which crashes in this solver on
+  rows of 4+ words).  Matrices are regenerated from their seeds at test time
   (xorshift64 Bernoulli fill, see oracle/bmm_oracle.c:orc_gen_instance).
 """
 
@@ -37,12 +41,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-from oracle.oracle import port, ref  # noqa: E402
+from oracle.oracle import port, ref, ref_scalar  # noqa: E402
 from oracle.oracle import ga_config  # noqa: E402
 from tests.golden.fixtures import (  # noqa: E402
     C1,
     C2,
     C3,
+    BASIS_CASES,
     GA_CASES,
     batch_instance,
     cuda_equivalence_matrix,
@@ -104,7 +109,7 @@ def per_target(R, m, cols, rows, k, offset=1):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-slow", action="store_true")
-    ap.add_argument("--only", default="", help="comma list of c1,c2,c3,c4,ga,ka to regenerate; "
+    ap.add_argument("--only", default="", help="comma list of c1,c2,c3,c4,ga,basis,ka to regenerate; "
                     "the other entries of workloads.npz are kept")
     args = ap.parse_args()
     only = set(filter(None, args.only.split(",")))
@@ -135,6 +140,8 @@ def main():
         c3(R, P, arrays)
     if want("ga"):
         ga(R, P, arrays)
+    if want("basis"):
+        basis(ref_scalar(), P, arrays)
     np.savez_compressed(npz, **arrays)
     print("workloads.npz written")
 
@@ -200,6 +207,23 @@ def ga(R, P, arrays):
         arrays[f"ga{i}_weights"] = bw
         print(f"  GA case {i}: {len(scores) - 1} steps, best {scores[-1]}, {secs:.2f}s")
     print("GA done", time.time() - t0)
+
+
+def basis(R, P, arrays):
+    t0 = time.time()
+    for i, (rows, cols, p, iseed, scr, win) in enumerate(BASIS_CASES):
+        m, _ = P.gen_instance(rows, cols, p, iseed, scr)
+        r = R.exact_basis(m, cols, win)
+        arrays[f"basis{i}_masks"] = np.array(r["basis_masks"], np.uint32)
+        arrays[f"basis{i}_weights"] = np.array(r["basis_weights"], np.uint32)
+        arrays[f"basis{i}_transform"] = np.array(r["transform"], np.uint64)
+        arrays[f"basis{i}_scalars"] = np.array(
+            [r["input_rows"], r["cols"], r["rank"], r["enumerated_states"], r["total_weight"]],
+            np.uint64)
+        if cols <= 4096:
+            arrays[f"basis{i}_words"] = r["basis_words"]
+        print(f"  basis case {i}: rank {r['rank']}, total {r['total_weight']}")
+    print("basis done", time.time() - t0)
 
 
 if __name__ == "__main__":
