@@ -162,6 +162,8 @@ SIGNATURES = {
     "bmm_exact_basis": [_u64p, _sz, _sz, _u32p, _sz, C.POINTER(ExactBasisConfig_t),
                         C.POINTER(ExactBasisResult_t), _u32p, _u32p],
     "bmm_basis_weight_counts": [_u64p, _sz, _sz, _u32p, _sz, _u64p],
+    "bmm_basis_weight_counts_dev": [_vp, _sz, _sz, _vp, _vp],
+    "bmm_basis_tune": [C.c_int],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
              "bmm_gen_instance": C.c_uint64, "bmm_mlp_param_count": C.c_size_t}

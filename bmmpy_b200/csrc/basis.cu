@@ -9,14 +9,16 @@
 // only on the order in which candidates are offered, so this version keeps
 // the order and changes everything else:
 //
-//  * enumeration on the device.  G lanes share one prefix of the high `hb`
-//    mask bits, each holding WPL words of the running XOR in registers (the
-//    window rows staged in shared memory); a prefix sweeps its 2^chunk low
-//    bits in Gray order.  Pass 0 builds the weight histogram (per-CTA shared
-//    bins), pass 1 collects the combinations whose weight lies in [lo, hi]
-//    as keys (weight << 32) | enumeration index, which sorted ascending are
-//    the reference's bucket order.  Windows wider than 64 words per lane x 32
-//    lanes accumulate per-mask weights slab by slab instead.
+//  * enumeration on the device, in the reference's own Gray walk: state k
+//    (1 <= k < 2^t) is mask k ^ (k >> 1), reached from k - 1 by toggling row
+//    ctz(k).  One wave of CTAs (one per resident slot) cuts the walk into
+//    equal contiguous slices, one per group of G lanes; each lane holds WPL
+//    words of the running XOR in registers, the window rows sit in shared
+//    memory.  Pass 0 builds the weight histogram (per-CTA shared bins), pass
+//    1 collects the states whose weight lies in [lo, hi] as keys
+//    (weight << 32) | k, which sorted ascending are the reference's bucket
+//    order.  Windows wider than 64 words per lane x 32 lanes accumulate
+//    per-mask weights slab by slab instead.
 //  * the greedy on r-bit coordinates.  Projecting the row space onto the
 //    pivot columns of an echelon form of the window is an isomorphism, so a
 //    combination's coordinate is the XOR of its rows' coordinates (four byte
@@ -24,8 +26,10 @@
 //  * only as many candidates as the greedy consumes: the weight cut starts
 //    where the histogram holds 4r nonzero candidates and grows 4x per pass.
 #include "common.cuh"
+#include "popc.cuh"
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 namespace bmm {
@@ -38,9 +42,20 @@ constexpr int kMaxGroup = 32;     // lanes per prefix (one warp)
 
 enum Mode : int { kHist = 0, kCollect = 1, kAccumulate = 2 };
 
+// Histogram increments as fire-and-forget reductions.  The asm carries no
+// memory clobber on purpose: the bins never alias the window rows in shared
+// memory, and without a clobber the compiler may issue the next step's row
+// loads ahead of this update instead of serialising every step behind it.
+__device__ __forceinline__ void red_shared_add(unsigned* p, unsigned v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" ::"r"((unsigned)__cvta_generic_to_shared(p)),
+                 "r"(v));
+}
+
 struct Launch {
-    const uint64_t* rows;  // t x W words (one column slab in kAccumulate)
-    int t, W, cols, G, hb, chunk, mode;
+    const uint64_t* rows;  // t rows of W words, `pitch` words apart (a column slab)
+    size_t pitch;
+    int t, W, cols, mode;
+    uint32_t L;                     // states per lane group (a multiple of 32)
     uint32_t lo, hi;                // kCollect: weight range
     unsigned long long* counts;     // kHist: cols + 1 bins
     unsigned long long* keys;       // kCollect
@@ -50,87 +65,110 @@ struct Launch {
     int first;                      // kAccumulate: first slab stores, later slabs add
 };
 
-template <int WPL>
+// Shared layout of the window rows: lane gl of a group owns words
+// [gl * WPL, (gl + 1) * WPL) of every row, stored in VEC-word chunks
+// interleaved across the group -- chunk q of lane gl of row b at
+// ((b * Q + q) * G + gl) -- so the G lanes of a group read adjacent chunks
+// (the groups of a warp read the same row at the same step, a broadcast,
+// except where their slices' counters differ in a bit >= 5).
+template <int WPL, int G, int NHB>
 __global__ void __launch_bounds__(kThreads) enum_kernel(const Launch a) {
+    constexpr int VEC = WPL >= 2 ? 2 : 1;  // words per shared load
+    constexpr int Q = WPL / VEC;
+    using Vec = typename std::conditional<VEC == 2, ulonglong2, unsigned long long>::type;
     extern __shared__ __align__(16) unsigned char smem[];
-    uint64_t* srow = reinterpret_cast<uint64_t*>(smem);  // t x (G * WPL) words
-    const int SW = a.G * WPL;
-    unsigned* hist = reinterpret_cast<unsigned*>(srow + (size_t)a.t * SW);
+    Vec* srow = reinterpret_cast<Vec*>(smem);  // t x Q x G chunks
+    const int SW = G * WPL;
+    unsigned* hist = reinterpret_cast<unsigned*>(smem + (size_t)a.t * SW * 8);
     const bool shared_hist = a.mode == kHist && a.cols + 1 <= kHistSmem;
+    uint64_t* sw = reinterpret_cast<uint64_t*>(smem);
     for (int i = threadIdx.x; i < a.t * SW; i += blockDim.x) {
-        const int r = i / SW, w = i % SW;
-        srow[i] = w < a.W ? a.rows[(size_t)r * a.W + w] : 0ull;
+        const int r = i / SW, w = i % SW;  // word w of row r
+        const int gl = w / WPL, k = w % WPL, q = k / VEC, v = k % VEC;
+        sw[(((size_t)r * Q + q) * G + gl) * VEC + v] =
+            w < a.W ? a.rows[(size_t)r * a.pitch + w] : 0ull;
     }
     if (shared_hist)
         for (int i = threadIdx.x; i <= a.cols; i += blockDim.x)
             hist[i] = 0;
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int gl = lane % a.G;  // lane within the group
-    const unsigned long long p =
-        ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) / a.G;
-    const bool valid = p < (1ull << a.hb);
+    const int gl = lane % G;  // lane within the group
     uint64_t cur[WPL];
 #pragma unroll
     for (int i = 0; i < WPL; ++i)
         cur[i] = 0;
-    if (valid)
-        for (int b = 0; b < a.hb; ++b)
-            if ((p >> b) & 1ull)
+    auto toggle = [&](int b) {
+        const Vec* src = srow + (size_t)b * Q * G + gl;
 #pragma unroll
-                for (int i = 0; i < WPL; ++i)
-                    cur[i] ^= srow[(size_t)(a.chunk + b) * SW + gl * WPL + i];
-    const uint32_t hi_bits = (uint32_t)(p << a.chunk);
-    // enumeration index of mask hi|gray(s): inverse Gray of the high part on
-    // top, and s itself, complemented when the high part has odd parity
-    const uint32_t idx_hi = (uint32_t)(inverse_gray64(p) << a.chunk);
-    const uint32_t low_flip = (__popcll(p) & 1) ? ((1u << a.chunk) - 1) : 0u;
-    uint32_t low = 0;
-    const uint32_t states = 1u << a.chunk;
-    for (uint32_t s = 0; s < states; ++s) {
-        if (s) {
-            const int b = __ffs(s) - 1;
-#pragma unroll
-            for (int i = 0; i < WPL; ++i)
-                cur[i] ^= srow[(size_t)b * SW + gl * WPL + i];
-            low ^= 1u << b;
+        for (int q = 0; q < Q; ++q) {
+            const Vec x = src[q * G];
+            if constexpr (VEC == 2) {
+                cur[2 * q] ^= x.x;
+                cur[2 * q + 1] ^= x.y;
+            } else {
+                cur[q] ^= x;
+            }
         }
-        uint32_t w = 0;
-#pragma unroll
-        for (int i = 0; i < WPL; ++i)
-            w += __popcll(cur[i]);
-        for (int o = a.G >> 1; o > 0; o >>= 1)
-            w += __shfl_xor_sync(kFull, w, o);
-        const uint32_t mask = hi_bits | low;
-        const bool lead = valid && gl == 0;
+    };
+    // this group's slice [k0, k0 + n) of the Gray walk k -> mask k ^ (k >> 1);
+    // only the last groups have n < L (n = 0 past the end)
+    const unsigned long long total = 1ull << a.t;
+    const unsigned long long k0 =
+        ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) / G * a.L;
+    const uint32_t n = k0 < total ? (uint32_t)min((unsigned long long)a.L, total - k0) : 0u;
+    const unsigned gmask = G == 32 ? kFull : ((1u << G) - 1) << (lane & ~(G - 1));
+    auto emit = [&](unsigned long long k, uint32_t w) {
+        if (gl != 0 || k == 0)
+            return;
         if (a.mode == kHist) {
-            if (lead && mask != 0) {
-                if (shared_hist)
-                    atomicAdd(hist + w, 1u);
-                else
-                    atomicAdd(a.counts + w, 1ull);
-            }
+            if (shared_hist)
+                red_shared_add(hist + w, 1u);
+            else
+                atomicAdd(a.counts + w, 1ull);
         } else if (a.mode == kCollect) {
-            const bool hit = lead && mask != 0 && w >= a.lo && w <= a.hi;
-            const unsigned bal = __ballot_sync(kFull, hit);
-            if (bal) {
-                unsigned long long base = 0;
-                if (lane == __ffs(bal) - 1)
-                    base = atomicAdd(a.nkeys, (unsigned long long)__popc(bal));
-                base = __shfl_sync(kFull, base, __ffs(bal) - 1);
-                if (hit) {
-                    const unsigned long long pos = base + __popc(bal & ((1u << lane) - 1));
-                    if (pos < a.cap)
-                        a.keys[pos] =
-                            ((unsigned long long)w << 32) | (idx_hi | (s ^ low_flip));
-                }
+            if (w >= a.lo && w <= a.hi) {
+                const unsigned long long pos = atomicAdd(a.nkeys, 1ull);
+                if (pos < a.cap)
+                    a.keys[pos] = ((unsigned long long)w << 32) | (uint32_t)k;
             }
-        } else if (lead) {
+        } else {
+            const uint32_t mask = (uint32_t)(k ^ (k >> 1));
             if (a.first)
                 a.weights[mask] = w;
             else
                 a.weights[mask] += w;
         }
+    };
+    if (n) {
+        uint32_t g0 = (uint32_t)(k0 ^ (k0 >> 1));
+        while (g0) {
+            toggle(__ffs(g0) - 1);
+            g0 &= g0 - 1;
+        }
+        uint32_t w = 0;
+#pragma unroll
+        for (int i = 0; i < WPL; ++i)
+            w += __popcll(cur[i]);
+        for (int o = G >> 1; o > 0; o >>= 1)
+            w += __shfl_xor_sync(gmask, w, o);
+        emit(k0, w);
+    }
+    for (uint32_t j = 1; j < n; ++j) {
+        // k0 and L are multiples of 32: the toggled row is ctz(j) unless j is
+        // a multiple of 32 too, so it is warp-uniform 31 steps in 32
+        const unsigned long long k = k0 + j;
+        const int b = (j & 31) ? __ffs(j) - 1 : __ffsll((long long)k) - 1;
+        uint32_t w;
+        if constexpr (VEC == 2) {
+            w = xor_row_popc_hs<WPL, NHB>(cur, sw + ((size_t)b * Q * G + gl) * 2, G);
+        } else {
+            toggle(b);
+            w = __popcll(cur[0]);
+        }
+        for (int o = G >> 1; o > 0; o >>= 1)
+            w += __shfl_xor_sync(gmask, w, o);
+        emit(k, w);
     }
     if (shared_hist) {
         __syncthreads();
@@ -176,13 +214,12 @@ __global__ void weights_collect_kernel(const uint32_t* __restrict__ weights,
 }
 
 struct Plan {
-    int G, wpl, hb, chunk;
-    long long blocks;
+    int G, wpl;
     size_t smem;
 };
 
 // W: words per row handled by one launch (the whole row, or one slab).
-Plan plan_for(int t, int W, int cols, int sm_count) {
+Plan plan_for(int t, int W, int cols) {
     Plan p{};
     p.G = 1;
     while ((W + p.G - 1) / p.G > kMaxWpl)
@@ -191,52 +228,80 @@ Plan plan_for(int t, int W, int cols, int sm_count) {
     p.wpl = 1;
     while (p.wpl < need)
         p.wpl <<= 1;
-    // prefixes for about 8 CTAs of 128 threads per SM, each sweeping at least
-    // 2^min(6, t) states, and chunk <= 31 so a sweep counts in 32 bits
-    const long long want = (long long)sm_count * 8 * kThreads / p.G;
-    int hb = 0;
-    while (hb < t && (2ll << hb) <= want && t - (hb + 1) >= std::min(6, t))
-        ++hb;
-    if (t - hb > 31)
-        hb = t - 31;
-    p.hb = hb;
-    p.chunk = t - hb;
-    const long long threads = (1ll << hb) * p.G;
-    p.blocks = (threads + kThreads - 1) / kThreads;
-    p.smem = (size_t)t * p.G * p.wpl * 8 + (size_t)(cols + 1 <= kHistSmem ? (cols + 1) * 4 : 0);
     // G * WPL is the power of two at or above W, and W <= slab_words(t)
+    p.smem = (size_t)t * p.G * p.wpl * 8 + (size_t)(cols + 1 <= kHistSmem ? (cols + 1) * 4 : 0);
     return p;
 }
 
-int launch(const Plan& pl, Launch a, cudaStream_t s) {
-    a.G = pl.G;
-    a.hb = pl.hb;
-    a.chunk = pl.chunk;
-#define BMM_ENUM(N)                                                                               \
-    case N: {                                                                                     \
-        auto k = enum_kernel<N>;                                                                  \
-        BMM_CUDA_TRY(                                                                             \
-            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.smem));  \
-        k<<<(unsigned)pl.blocks, kThreads, pl.smem, s>>>(a);                                      \
-        BMM_CUDA_TRY(cudaGetLastError());                                                         \
-        return BMM_OK;                                                                            \
+// One CTA per resident slot (a single wave); the 2^t states are cut into
+// equal contiguous slices of the Gray walk, one per lane group, each a
+// multiple of 32 states long.
+template <typename K>
+int launch_kernel(K kernel, const Plan& pl, Launch a, int sm_count, cudaStream_t s) {
+    BMM_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)pl.smem));
+    int per_sm = 0;
+    BMM_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads,
+                                                               pl.smem));
+    if (per_sm < 1)
+        return fail(BMM_EINVAL, "exact basis: kernel does not fit on an SM");
+    const unsigned long long total = 1ull << a.t;
+    const unsigned long long groups = (unsigned long long)per_sm * sm_count * kThreads / pl.G;
+    unsigned long long L = (total + groups - 1) / groups;
+    L = std::max<unsigned long long>(32, (L + 31) / 32 * 32);
+    const unsigned long long used = (total + L - 1) / L;  // groups with work
+    const unsigned blocks = (unsigned)((used * pl.G + kThreads - 1) / kThreads);
+    a.L = (uint32_t)L;
+    kernel<<<blocks, kThreads, pl.smem, s>>>(a);
+    BMM_CUDA_TRY(cudaGetLastError());
+    return BMM_OK;
+}
+
+int g_basis_nhb = -1;  // carry-save blocks per 64-word lane; -1 = default_nhb
+
+template <int WPL, int G>
+int launch_g(const Plan& pl, const Launch& a, int sm_count, cudaStream_t s) {
+    if constexpr (WPL == 64) {
+        switch (g_basis_nhb) {
+        case 0: return launch_kernel(enum_kernel<64, G, 0>, pl, a, sm_count, s);
+        case 2: return launch_kernel(enum_kernel<64, G, 2>, pl, a, sm_count, s);
+        case 8: return launch_kernel(enum_kernel<64, G, 8>, pl, a, sm_count, s);
+        default: break;
+        }
     }
-    switch (pl.wpl) {
-        BMM_ENUM(1)
-        BMM_ENUM(2)
-        BMM_ENUM(4)
-        BMM_ENUM(8)
-        BMM_ENUM(16)
-        BMM_ENUM(32)
-        BMM_ENUM(64)
+    // rows of 8+ lanes per group favour the full carry-save tree (measured)
+    constexpr int nhb = (WPL == 64 && G >= 8) ? 8 : default_nhb(WPL);
+    return launch_kernel(enum_kernel<WPL, G, nhb>, pl, a, sm_count, s);
+}
+
+// G > 1 only when one lane's share is above 32 words, i.e. WPL == 64.
+int launch(const Plan& pl, Launch a, int sm_count, cudaStream_t s) {
+    if (pl.wpl == 64) {
+        switch (pl.G) {
+        case 1: return launch_g<64, 1>(pl, a, sm_count, s);
+        case 2: return launch_g<64, 2>(pl, a, sm_count, s);
+        case 4: return launch_g<64, 4>(pl, a, sm_count, s);
+        case 8: return launch_g<64, 8>(pl, a, sm_count, s);
+        case 16: return launch_g<64, 16>(pl, a, sm_count, s);
+        case 32: return launch_g<64, 32>(pl, a, sm_count, s);
+        }
+    } else if (pl.G == 1) {
+        switch (pl.wpl) {
+        case 1: return launch_g<1, 1>(pl, a, sm_count, s);
+        case 2: return launch_g<2, 1>(pl, a, sm_count, s);
+        case 4: return launch_g<4, 1>(pl, a, sm_count, s);
+        case 8: return launch_g<8, 1>(pl, a, sm_count, s);
+        case 16: return launch_g<16, 1>(pl, a, sm_count, s);
+        case 32: return launch_g<32, 1>(pl, a, sm_count, s);
+        }
     }
-#undef BMM_ENUM
     return fail(BMM_EINVAL, "exact basis: unsupported row width");
 }
 
 // Widest row slab one launch handles: G * WPL words per row for all t rows
 // in shared memory (at most 192 KB; cols < 16384 also keeps a 64 KB histogram,
-// and those rows are at most 256 words).
+// and those rows are at most 256 words).  Wider windows run one launch per
+// slab, adding each slab's popcounts into a per-mask weight array.
 size_t slab_words(int t) {
     size_t s = (size_t)kMaxWpl * kMaxGroup;
     while (s > 1 && (size_t)t * s * 8 > 196608)
@@ -248,91 +313,97 @@ size_t slab_words(int t) {
 // per-mask weights for wide windows, histogram and ranged collection.
 struct Enumerator {
     Workspace* ws = nullptr;
+    cudaStream_t stream = nullptr;
     int t = 0, cols = 0;
     size_t W = 0, slab = 0;
-    uint64_t* d_rows = nullptr;
+    const uint64_t* d_rows = nullptr;
     uint32_t* d_weights = nullptr;  // wide windows only
     unsigned long long states = 0;
 
     bool wide() const { return W > slab; }
 
-    int init(Workspace* w, const uint64_t* words, size_t stride, size_t ncols,
-             const uint32_t* win, size_t nt) {
+    // Window rows (t x W words, row-major, tail bits clear) already on the device.
+    int init_dev(Workspace* w, const uint64_t* rows_dev, size_t ncols, size_t nt,
+                 cudaStream_t st) {
         ws = w;
+        stream = st;
         t = (int)nt;
         cols = (int)ncols;
         W = (ncols + 63) / 64;
         slab = slab_words(t);
         states = (1ull << nt) - 1;
-        const size_t slabs = (W + slab - 1) / slab;
-        // narrow: row r at r * W; wide: slab j of row r at (j * t + r) * slab
-        std::vector<uint64_t> h(wide() ? slabs * nt * slab : nt * std::max<size_t>(W, 1), 0ull);
-        const uint64_t tail = (ncols & 63) ? ((1ull << (ncols & 63)) - 1) : ~0ull;
-        for (size_t r = 0; r < nt; ++r)
-            for (size_t c = 0; c < W; ++c) {
-                const uint64_t v = words[(size_t)win[r] * stride + c] & (c == W - 1 ? tail : ~0ull);
-                if (wide())
-                    h[((c / slab) * nt + r) * slab + c % slab] = v;
-                else
-                    h[r * W + c] = v;
-            }
-        void* p = nullptr;
-        BMM_TRY(ws_buffer(ws, kSlotRows, h.size() * 8, &p));
-        BMM_CUDA_TRY(cudaMemcpyAsync(p, h.data(), h.size() * 8, cudaMemcpyHostToDevice,
-                                     ws->stream));
-        d_rows = (uint64_t*)p;
+        d_rows = rows_dev;
         if (wide()) {
             void* q = nullptr;
             BMM_TRY(ws_buffer(ws, kSlotExtra0, (size_t)(states + 1) * 4, &q));
             d_weights = (uint32_t*)q;
-            const Plan pl = plan_for(t, (int)slab, cols, ws->sm_count);
-            for (size_t j = 0; j < slabs; ++j) {
+            const Plan pl = plan_for(t, (int)slab, cols);
+            for (size_t j = 0; j * slab < W; ++j) {
                 Launch a{};
-                a.rows = d_rows + j * nt * slab;
+                a.rows = d_rows + j * slab;
+                a.pitch = W;
                 a.t = t;
-                a.W = (int)slab;
+                a.W = (int)std::min(slab, W - j * slab);
                 a.cols = cols;
                 a.mode = kAccumulate;
                 a.weights = d_weights;
                 a.first = j == 0;
-                BMM_TRY(launch(pl, a, ws->stream));
+                BMM_TRY(launch(pl, a, ws->sm_count, stream));
             }
         }
         return BMM_OK;
     }
 
+    // Window rows gathered from a host matrix.
+    int init(Workspace* w, const uint64_t* words, size_t stride, size_t ncols,
+             const uint32_t* win, size_t nt) {
+        const size_t nw = (ncols + 63) / 64;
+        std::vector<uint64_t> h(nt * std::max<size_t>(nw, 1), 0ull);
+        const uint64_t tail = (ncols & 63) ? ((1ull << (ncols & 63)) - 1) : ~0ull;
+        for (size_t r = 0; r < nt; ++r)
+            for (size_t c = 0; c < nw; ++c)
+                h[r * nw + c] = words[(size_t)win[r] * stride + c] & (c == nw - 1 ? tail : ~0ull);
+        void* p = nullptr;
+        BMM_TRY(ws_buffer(w, kSlotRows, h.size() * 8, &p));
+        BMM_CUDA_TRY(cudaMemcpyAsync(p, h.data(), h.size() * 8, cudaMemcpyHostToDevice,
+                                     w->stream));
+        return init_dev(w, (const uint64_t*)p, ncols, nt, w->stream);
+    }
+
     int hist(unsigned long long* d_counts) {
-        BMM_CUDA_TRY(cudaMemsetAsync(d_counts, 0, ((size_t)cols + 1) * 8, ws->stream));
+        BMM_CUDA_TRY(cudaMemsetAsync(d_counts, 0, ((size_t)cols + 1) * 8, stream));
         if (wide()) {
             const unsigned blocks = (unsigned)std::min<unsigned long long>(
                 (states + 255) / 256, (unsigned long long)ws->sm_count * 16);
-            weights_hist_kernel<<<blocks, 256, 0, ws->stream>>>(d_weights, states, d_counts);
+            weights_hist_kernel<<<blocks, 256, 0, stream>>>(d_weights, states, d_counts);
             BMM_CUDA_TRY(cudaGetLastError());
             return BMM_OK;
         }
         Launch a{};
         a.rows = d_rows;
+        a.pitch = W;
         a.t = t;
         a.W = (int)W;
         a.cols = cols;
         a.mode = kHist;
         a.counts = d_counts;
-        return launch(plan_for(t, (int)W, cols, ws->sm_count), a, ws->stream);
+        return launch(plan_for(t, (int)W, cols), a, ws->sm_count, stream);
     }
 
     int collect(uint32_t lo, uint32_t hi, unsigned long long* d_keys, unsigned long long cap,
                 unsigned long long* d_n) {
-        BMM_CUDA_TRY(cudaMemsetAsync(d_n, 0, 8, ws->stream));
+        BMM_CUDA_TRY(cudaMemsetAsync(d_n, 0, 8, stream));
         if (wide()) {
             const unsigned blocks = (unsigned)std::min<unsigned long long>(
                 (states + 256) / 256, (unsigned long long)ws->sm_count * 16);
-            weights_collect_kernel<<<blocks, 256, 0, ws->stream>>>(d_weights, states, lo, hi,
-                                                                   d_keys, d_n, cap);
+            weights_collect_kernel<<<blocks, 256, 0, stream>>>(d_weights, states, lo, hi, d_keys,
+                                                               d_n, cap);
             BMM_CUDA_TRY(cudaGetLastError());
             return BMM_OK;
         }
         Launch a{};
         a.rows = d_rows;
+        a.pitch = W;
         a.t = t;
         a.W = (int)W;
         a.cols = cols;
@@ -342,7 +413,7 @@ struct Enumerator {
         a.keys = d_keys;
         a.nkeys = d_n;
         a.cap = cap;
-        return launch(plan_for(t, (int)W, cols, ws->sm_count), a, ws->stream);
+        return launch(plan_for(t, (int)W, cols), a, ws->sm_count, stream);
     }
 };
 
@@ -428,6 +499,32 @@ BMM_API int bmm_basis_weight_counts(const uint64_t* words, size_t stride, size_t
                                  ws->stream));
     BMM_CUDA_TRY(cudaStreamSynchronize(ws->stream));
     return BMM_OK;
+}
+
+BMM_API int bmm_basis_tune(int hs_blocks) {
+    clear_error();
+    if (hs_blocks != -1 && hs_blocks != 0 && hs_blocks != 2 && hs_blocks != 5 && hs_blocks != 8)
+        return fail(BMM_EINVAL, "basis tuning: hs_blocks must be -1, 0, 2, 5 or 8");
+    basis::g_basis_nhb = hs_blocks == 5 ? -1 : hs_blocks;
+    return BMM_OK;
+}
+
+BMM_API int bmm_basis_weight_counts_dev(const uint64_t* rows, size_t t, size_t cols,
+                                        uint64_t* counts, void* stream) {
+    clear_error();
+    if (!rows || !counts)
+        return fail(BMM_EINVAL, "exact basis: null device pointer");
+    if (t == 0 || t > 32)
+        return fail(BMM_EINVAL, "exact basis: window rows must be in [1, 32]");
+    if (cols >= (1ull << 31))
+        return fail(BMM_EINVAL, "exact basis: too many columns");
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    basis::Enumerator en;
+    BMM_TRY(en.init_dev(ws, rows, cols, t, (cudaStream_t)stream));
+    return en.hist((unsigned long long*)counts);
 }
 
 BMM_API int bmm_exact_basis(const uint64_t* words, size_t stride, size_t cols,

@@ -17,6 +17,7 @@
 // min folded with one 64-bit atomicMin per warp.
 #include "common.cuh"
 #include "gray.cuh"
+#include "popc.cuh"
 #include "topk.cuh"
 
 #include <mutex>
@@ -37,76 +38,6 @@ __device__ __forceinline__ uint32_t xor_row_popc(uint64_t (&cur)[WPL], const uin
         cur[2 * i + 1] ^= v.y;
         s += __popcll(cur[2 * i]) + __popcll(cur[2 * i + 1]);
     }
-    return s;
-}
-
-// Carry-save adder: l = a ^ b ^ c (weight 1), h = majority(a, b, c) (weight 2).
-__device__ __forceinline__ void csa(uint32_t& h, uint32_t& l, uint32_t a, uint32_t b, uint32_t c) {
-    const uint32_t u = a ^ b;
-    h = (a & b) | (u & c);
-    l = u ^ c;
-}
-
-// Harley-Seal step over 16 words (Mula, Kurz, Lemire, "Faster population
-// counts using AVX2 instructions", 2018): 15 carry-save adders fold the block
-// into running ones/twos/fours/eights and emit one "sixteens" word, so 16
-// words cost 30 LOP3 + 1 POPC instead of 16 POPC.
-__device__ __forceinline__ void hs16(const uint32_t (&d)[16], uint32_t& ones, uint32_t& twos,
-                                     uint32_t& fours, uint32_t& eights, uint32_t& n16) {
-    uint32_t twosA, twosB, foursA, foursB, eightsA, eightsB, sixteens;
-    csa(twosA, ones, ones, d[0], d[1]);
-    csa(twosB, ones, ones, d[2], d[3]);
-    csa(foursA, twos, twos, twosA, twosB);
-    csa(twosA, ones, ones, d[4], d[5]);
-    csa(twosB, ones, ones, d[6], d[7]);
-    csa(foursB, twos, twos, twosA, twosB);
-    csa(eightsA, fours, fours, foursA, foursB);
-    csa(twosA, ones, ones, d[8], d[9]);
-    csa(twosB, ones, ones, d[10], d[11]);
-    csa(foursA, twos, twos, twosA, twosB);
-    csa(twosA, ones, ones, d[12], d[13]);
-    csa(twosB, ones, ones, d[14], d[15]);
-    csa(foursB, twos, twos, twosA, twosB);
-    csa(eightsB, fours, fours, foursA, foursB);
-    csa(sixteens, eights, eights, eightsA, eightsB);
-    n16 += __popc(sixteens);
-}
-
-// XOR a shared-memory row into cur and return popcount(cur).  The first
-// NHB blocks of 8 words go through the carry-save tree (ALU pipe), the rest
-// through POPC (XU pipe); NHB balances the two pipes.
-template <int WPL, int NHB>
-__device__ __forceinline__ uint32_t xor_row_popc_hs(uint64_t (&cur)[WPL], const uint64_t* srow) {
-    static_assert(NHB * 8 <= WPL, "carry-save blocks exceed the row");
-    const ulonglong2* p = reinterpret_cast<const ulonglong2*>(srow);
-    uint32_t ones = 0, twos = 0, fours = 0, eights = 0, n16 = 0;
-#pragma unroll
-    for (int blk = 0; blk < NHB; ++blk) {
-        uint32_t d[16];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const ulonglong2 v = p[blk * 4 + j];
-            uint64_t& a = cur[blk * 8 + 2 * j];
-            uint64_t& b = cur[blk * 8 + 2 * j + 1];
-            a ^= v.x;
-            b ^= v.y;
-            d[4 * j + 0] = (uint32_t)a;
-            d[4 * j + 1] = (uint32_t)(a >> 32);
-            d[4 * j + 2] = (uint32_t)b;
-            d[4 * j + 3] = (uint32_t)(b >> 32);
-        }
-        hs16(d, ones, twos, fours, eights, n16);
-    }
-    uint32_t s = 0;
-#pragma unroll
-    for (int i = NHB * 4; i < WPL / 2; ++i) {
-        const ulonglong2 v = p[i];
-        cur[2 * i] ^= v.x;
-        cur[2 * i + 1] ^= v.y;
-        s += __popcll(cur[2 * i]) + __popcll(cur[2 * i + 1]);
-    }
-    if (NHB > 0)
-        s += 16 * n16 + 8 * __popc(eights) + 4 * __popc(fours) + 2 * __popc(twos) + __popc(ones);
     return s;
 }
 
@@ -311,7 +242,6 @@ __global__ void decode_keys_kernel(const unsigned long long* __restrict__ keys, 
 // the XU pipe (POPC) saturates while ALU idles at ~36 %; 5 of the 8 blocks of
 // a 64-word lane through the adder tree measured fastest on B200 (40 x 4096,
 // k = 24: 20.3 ms -> 15.7 ms per step); narrower lanes keep the same ratio.
-constexpr int default_nhb(int wpl) { return wpl >= 64 ? 5 : wpl >= 32 ? 2 : wpl >= 16 ? 1 : 0; }
 
 int group_shape(size_t W, int* wpl, int* g) {
     if (W <= 2) {

@@ -409,6 +409,17 @@ BMM_API int bmm_exact_basis(const uint64_t* words, size_t stride, size_t cols,
 BMM_API int bmm_basis_weight_counts(const uint64_t* words, size_t stride, size_t cols,
                                     const uint32_t* win, size_t t, uint64_t* counts);
 
+/* Device form: `rows` holds the t window rows (1 <= t <= 32) row-major,
+ * (cols + 63) / 64 words each with the bits at and past `cols` clear; counts
+ * (cols + 1 entries) is overwritten on `stream`.  Asynchronous. */
+BMM_API int bmm_basis_weight_counts_dev(const uint64_t* rows, size_t t, size_t cols,
+                                        uint64_t* counts, void* stream);
+
+/* Autotuner hook for the enumeration kernel (no reference counterpart):
+ * carry-save blocks of 8 words per 64-word lane (0, 2, 5 or 8; -1 = built-in
+ * policy).  Process-wide; results never change, only speed. */
+BMM_API int bmm_basis_tune(int hs_blocks);
+
 #ifdef __cplusplus
 }
 #endif
