@@ -31,6 +31,10 @@ only).
 of the planted 256 x 8192 matrix: ``value`` from the device histogram pass on
 resident rows, ``e2e`` from the public solve() on host windows.
 
+``--workload sa`` (1 GPU) measures SASelector (pairwise synergy, defaults) on
+the planted 512 x 65536 matrix: ``value`` from the device synergy table,
+``e2e`` from select().
+
 ``--workload ga`` (1 GPU) measures the island-model GA instead: the planted
 256 x 8192 matrix (density 0.01, 5000 scrambles, seed 7), 64 islands x 256,
 ring migration every 20 generations, stop at the planted weight or the
@@ -573,6 +577,129 @@ def run_basis(args):
     return 0
 
 
+SA_WINDOW = 32
+
+
+def _sa_config():
+    return {"workload": "SASelector(pairwise_synergy, 10000 iterations, 8 restarts, seed 1) "
+                        "choosing a 32-row window of the planted 512x65536 matrix (density 0.02, "
+                        "2000 scrambles, seed 2)",
+            "rows": C3["rows"], "cols": C3["cols"], "window": SA_WINDOW}
+
+
+def run_sa(args):
+    """SASelector: the device synergy table timed with CUDA events (value =
+    row-pair words/s), select() end to end from host memory (e2e), and the
+    reference selector on the same matrix as the CPU arm."""
+    from oracle.oracle import port, ref
+
+    words, _ = port().gen_instance(C3["rows"], C3["cols"], C3["p"], C3["seed"], C3["scrambles"])
+    if args.impl == "reference":
+        R = ref()
+        if R is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built"}))
+            return 0
+        per = []
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            R.sa_select(words, C3["cols"], SA_WINDOW, seed=1)
+            per.append(time.perf_counter() - t0)
+        v = len(per) / sum(per)
+        print(json.dumps({"impl": "reference", "metric": "SASelector.select calls/s", "value": v,
+                          "unit": "selections/s", "higher_is_better": True, "n_gpus": 0,
+                          "steps": len(per), "config": _sa_config(),
+                          "cpu_baseline": {"value": v, "unit": "selections/s", "cores": 1,
+                                           "kind": "reference",
+                                           "sample": f"{len(per)} selections"},
+                          "e2e": {"value": v, "unit": "selections/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0},
+                          "seconds_per_select": sum(per) / len(per)}), flush=True)
+        return 0
+    import ctypes
+
+    import torch
+
+    import bmmpy_b200 as bmm
+    from bmmpy_b200 import _native as N
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    m = bmm.BitMatrix(C3["rows"], C3["cols"])
+    m.words[:] = words[:, : m.stride_words]
+    rows, W = m.rows, m.words_per_row
+    d_words = torch.from_numpy(np.ascontiguousarray(m.words).view(np.int64)).to(dev)
+    d_table = torch.empty(rows * rows, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    L = N.lib()
+
+    def launch():
+        N.check(L.bmm_sa_pairwise_table_dev(d_words.data_ptr(), m.stride_words, rows, m.cols,
+                                            d_table.data_ptr(), stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        flush.zero_()
+        launch()
+    torch.cuda.synchronize()
+    sampler = clock_sampler(None)
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        launch()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    clocks = clock_summary(sampler)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    pair_words = rows * (rows - 1) // 2 * W
+    value = pair_words / (ms / 1e3)
+
+    selector = bmm.SASelector(seed=1)
+    first = selector.select(m, SA_WINDOW)
+    e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        res = selector.select(m, SA_WINDOW)
+    e_dt = (time.perf_counter() - t0) / e_steps
+    assert res.rows == first.rows
+
+    peak = ctypes.c_double(0)
+    N.check(L.bmm_probe_xor_popc(ctypes.byref(peak)))
+    line = {
+        "metric": "synergy-table row-pair words/s", "value": value, "unit": "words/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic planted matrix (xorshift64 seed 2)", "config": _sa_config(),
+        "e2e": {"value": 1.0 / e_dt, "unit": "selections/s",
+                "h2d_bytes_per_step": int(m.words.nbytes),
+                "d2h_bytes_per_step": int(rows * rows * 4),
+                "seconds_per_select": e_dt,
+                "note": "select(): device table + its D2H + the 80000-step chain on the host"},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "int-popc", "achieved": value / 1e9, "peak": peak.value / 1e9,
+                     "unit": "G words/s (64-bit AND+POPC)", "frac": value / peak.value,
+                     "peak_source": "measured in this run: register-only XOR+POPC probe kernel",
+                     "traffic": None},
+        "clocks": clocks,
+        "selected_rows": first.rows, "score": first.score,
+    }
+    if not args.no_cpu_baseline:
+        R = ref()
+        if R is not None:
+            t0 = time.perf_counter()
+            want = R.sa_select(words, C3["cols"], SA_WINDOW, seed=1)
+            dt = time.perf_counter() - t0
+            assert want["rows"] == first.rows and want["score"] == first.score
+            line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "selections/s", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": "one select(), reference SASelector (AVX2 build); "
+                                              "same rows and score as the GPU run"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -581,7 +708,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis"])
+    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa"])
     ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
     ap.add_argument("--seeds", type=int, default=2, help="GA: seeds per variant")
     ap.add_argument("--islands", type=int, default=64)
@@ -594,6 +721,8 @@ def main():
         return run_mitm(args)
     if args.workload == "basis":
         return run_basis(args)
+    if args.workload == "sa":
+        return run_sa(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

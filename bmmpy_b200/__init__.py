@@ -32,6 +32,8 @@ from .search import (
     CudaMitmFwhtSearch,
     FwhtSearch,
     MitmFwhtSearch,
+    SASelectionResult,
+    SASelector,
 )
 
 from .workflows import search_apply
@@ -57,6 +59,8 @@ __all__ = [
     "RunStats",
     "StopCriteria",
     "RowWindow",
+    "SASelectionResult",
+    "SASelector",
     "RuntimeFeatures",
     "fwht_i16",
     "fwht_i32",

@@ -112,6 +112,24 @@ class ExactBasisResult_t(C.Structure):
                 ("enumerated_states", C.c_uint64), ("total_weight", C.c_uint64)]
 
 
+class SaConfig_t(C.Structure):
+    """bmm_sa_config (SASelectorConfig)."""
+
+    _fields_ = [("iterations", C.c_uint64), ("restarts", C.c_uint64), ("seed", C.c_uint64),
+                ("score_policy", C.c_uint32), ("cooling_policy", C.c_uint32),
+                ("temperature_probe_samples", C.c_uint64),
+                ("initial_acceptance_probability", C.c_double), ("cooling_rate", C.c_double),
+                ("min_temperature", C.c_double)]
+
+
+class SaResult_t(C.Structure):
+    """bmm_sa_result (SASelectionResult without its rows)."""
+
+    _fields_ = [("score", C.c_int64), ("accepted_moves", C.c_uint64),
+                ("iterations_run", C.c_uint64), ("best_iteration", C.c_uint64),
+                ("restart_index", C.c_uint64), ("seed", C.c_uint64), ("n_rows", C.c_size_t)]
+
+
 # name -> argtypes (all return int unless listed in _RESTYPES)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
@@ -164,6 +182,10 @@ SIGNATURES = {
     "bmm_basis_weight_counts": [_u64p, _sz, _sz, _u32p, _sz, _u64p],
     "bmm_basis_weight_counts_dev": [_vp, _sz, _sz, _vp, _vp],
     "bmm_basis_tune": [C.c_int],
+    "bmm_sa_select": [_u64p, _sz, _sz, _sz, _sz, C.POINTER(SaConfig_t), C.POINTER(SaResult_t),
+                      _szp],
+    "bmm_sa_pairwise_table": [_u64p, _sz, _sz, _sz, _u32p],
+    "bmm_sa_pairwise_table_dev": [_vp, _sz, _sz, _sz, _vp, _vp],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
              "bmm_gen_instance": C.c_uint64, "bmm_mlp_param_count": C.c_size_t}

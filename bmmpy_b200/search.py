@@ -11,6 +11,9 @@ Cuda* classes keep the reference CUDA searchers' stricter argument checks
 (window of 16..64 rows, at most 128 candidates, brute-force widths of 512,
 1024 or 4096 columns, the int16-safe total weight for MITM) so that code and
 tests written against them behave identically.
+
+``SASelector`` (window selection by simulated annealing) mirrors the
+reference's selector of the same name.
 """
 
 from __future__ import annotations
@@ -203,3 +206,110 @@ class CudaBruteforceSearch:
                 "CudaBruteforceSearch: chunk_bits must be in [1, t - 1] or 0 for auto")
         return _run_window_search(N.lib().bmm_gray_search, window, self.max_candidates,
                                   self.max_candidates, self.chunk_bits)
+
+
+_SCORE_POLICIES = {"pairwise_synergy": 0, "higher_order_synergy": 1}
+_COOLING_POLICIES = {"adaptive_geometric": 0}
+
+
+def _resolve_score_policy(name: str) -> int:
+    if name in _SCORE_POLICIES:
+        return _SCORE_POLICIES[name]
+    raise ValueError(f"Unsupported score_policy: {name!r}")
+
+
+def _resolve_cooling_policy(name: str) -> int:
+    if name in _COOLING_POLICIES:
+        return _COOLING_POLICIES[name]
+    raise ValueError(f"Unsupported cooling_policy: {name!r}")
+
+
+class SASelectionResult:
+    """SASelectionResult (include/bmmpy/search/sa_selector.hpp:37-45)."""
+
+    __slots__ = ("rows", "score", "accepted_moves", "iterations_run", "best_iteration",
+                 "restart_index", "seed")
+
+    def __init__(self) -> None:
+        self.rows: list[int] = []
+        self.score = 0
+        self.accepted_moves = 0
+        self.iterations_run = 0
+        self.best_iteration = 0
+        self.restart_index = 0
+        self.seed = 0
+
+    def __repr__(self) -> str:
+        return (f"SASelectionResult(rows={self.rows}, score={self.score}, "
+                f"restart_index={self.restart_index})")
+
+
+class SASelector:
+    """Simulated-annealing window selection (bmmpy/search.py:416-537).
+
+    Same keyword arguments, checks, results and seed semantics as the reference:
+    the pairwise synergy table is built on the GPU and the annealing chain
+    (bmm_sa_select) replays the reference's generator stream exactly.
+    """
+
+    __slots__ = ("iterations", "restarts", "seed", "score_policy", "cooling_policy",
+                 "temperature_probe_samples", "initial_acceptance_probability", "cooling_rate",
+                 "min_temperature", "_cfg")
+
+    def __init__(self, *, iterations: int = 10000, restarts: int = 8, seed: int = 0,
+                 score_policy: str = "pairwise_synergy",
+                 cooling_policy: str = "adaptive_geometric",
+                 temperature_probe_samples: int = 64,
+                 initial_acceptance_probability: float = 0.8, cooling_rate: float = 0.99,
+                 min_temperature: float = 1e-6) -> None:
+        self._cfg = N.SaConfig_t(iterations, restarts, seed, _resolve_score_policy(score_policy),
+                                 _resolve_cooling_policy(cooling_policy),
+                                 temperature_probe_samples, initial_acceptance_probability,
+                                 cooling_rate, min_temperature)
+        self.iterations = iterations
+        self.restarts = restarts
+        self.seed = seed
+        self.score_policy = score_policy
+        self.cooling_policy = cooling_policy
+        self.temperature_probe_samples = temperature_probe_samples
+        self.initial_acceptance_probability = initial_acceptance_probability
+        self.cooling_rate = cooling_rate
+        self.min_temperature = min_temperature
+
+    def __repr__(self) -> str:
+        return ("SASelector("
+                f"iterations={self.iterations}, "
+                f"restarts={self.restarts}, "
+                f"seed={self.seed}, "
+                f"score_policy={self.score_policy!r}, "
+                f"cooling_policy={self.cooling_policy!r}, "
+                f"temperature_probe_samples={self.temperature_probe_samples}, "
+                f"initial_acceptance_probability={self.initial_acceptance_probability}, "
+                f"cooling_rate={self.cooling_rate}, "
+                f"min_temperature={self.min_temperature})")
+
+    def name(self) -> str:
+        return "sa"
+
+    def select(self, matrix, window_size: int) -> SASelectionResult:
+        """src/search/sa_selector.cpp:10-75."""
+        if window_size < 0:
+            raise ValueError("window_size must be non-negative")
+        res = N.SaResult_t()
+        rows = np.zeros(max(1, window_size), dtype=np.uintp)
+        words = np.ascontiguousarray(matrix.words)
+        N.check(N.lib().bmm_sa_select(N.u64p(words), matrix.stride_words, matrix.rows,
+                                      matrix.cols, window_size, self._cfg, res,
+                                      rows.ctypes.data_as(N._szp)), "bmm_sa_select")
+        out = SASelectionResult()
+        out.rows = [int(r) for r in rows[: res.n_rows]]
+        out.score = int(res.score)
+        out.accepted_moves = int(res.accepted_moves)
+        out.iterations_run = int(res.iterations_run)
+        out.best_iteration = int(res.best_iteration)
+        out.restart_index = int(res.restart_index)
+        out.seed = int(res.seed)
+        return out
+
+    def select_window(self, matrix, window_size: int) -> RowWindow:
+        return matrix.row_window(self.select(matrix, window_size).rows)

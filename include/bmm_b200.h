@@ -24,6 +24,9 @@
  *                        src/ga/genetic_algorithm_operators.cpp:15-192,
  *                        src/ga/genetic_algorithm_internal.hpp:41-103,
  *                        src/ga/island.cpp:149-228.
+ *   bmm_sa_select        SASelector::select  src/search/sa_selector.cpp:10-75,
+ *                        src/search/sa_selector_pairwise.cpp:21-172,
+ *                        src/search/sa_selector_higher_order.cpp:11-227.
  *   bmm_exact_basis      ExactBasisSolver::solve
  *                        src/solver/exact_basis_solver.cpp:58-157,
  *                        include/bmmpy/solver/exact_basis_solver.hpp:12-43.
@@ -414,6 +417,50 @@ BMM_API int bmm_basis_weight_counts(const uint64_t* words, size_t stride, size_t
  * (cols + 1 entries) is overwritten on `stream`.  Asynchronous. */
 BMM_API int bmm_basis_weight_counts_dev(const uint64_t* rows, size_t t, size_t cols,
                                         uint64_t* counts, void* stream);
+
+/* ---- simulated-annealing window selection ---------------------------------
+ * SASelectorConfig / SASelectionResult of include/bmmpy/search/sa_selector.hpp:14-45.
+ * score_policy: 0 PairwiseSynergy, 1 HigherOrderSynergy; cooling_policy:
+ * 0 AdaptiveGeometric. */
+typedef struct bmm_sa_config {
+    uint64_t iterations;                 /* reference default 10000 */
+    uint64_t restarts;                   /* 8 */
+    uint64_t seed;                       /* 0 -> 0x9E3779B97F4A7C15 */
+    uint32_t score_policy;
+    uint32_t cooling_policy;
+    uint64_t temperature_probe_samples;  /* 64 */
+    double initial_acceptance_probability; /* 0.8 */
+    double cooling_rate;                 /* 0.99 */
+    double min_temperature;              /* 1e-6 */
+} bmm_sa_config;
+
+typedef struct bmm_sa_result {
+    int64_t score;
+    uint64_t accepted_moves;
+    uint64_t iterations_run;
+    uint64_t best_iteration;
+    uint64_t restart_index;
+    uint64_t seed;
+    size_t n_rows;  /* rows written to out_rows (window_size, or 0) */
+} bmm_sa_result;
+
+/* SASelector::select (src/search/sa_selector.cpp:10-75) over a whole matrix of
+ * `rows` rows: the best window of window_size rows found by the reference's
+ * annealing chain (same generator stream, same result).  out_rows receives the
+ * sorted row indices.  The pairwise synergy table is built on the device; the
+ * chain runs on the calling thread.  Errors: the reference's messages. */
+BMM_API int bmm_sa_select(const uint64_t* words, size_t stride, size_t rows, size_t cols,
+                          size_t window_size, const bmm_sa_config* cfg, bmm_sa_result* res,
+                          size_t* out_rows);
+
+/* The pairwise synergy table of build_pairwise_synergy_table
+ * (src/search/sa_selector_pairwise.cpp:21-52): table[i * rows + j] =
+ * 2 * popc(row_i & row_j) for i != j, 0 on the diagonal.  Host form (rows^2
+ * uint32 out) and device form (asynchronous on `stream`). */
+BMM_API int bmm_sa_pairwise_table(const uint64_t* words, size_t stride, size_t rows, size_t cols,
+                                  uint32_t* table);
+BMM_API int bmm_sa_pairwise_table_dev(const uint64_t* words, size_t stride, size_t rows,
+                                      size_t cols, uint32_t* table, void* stream);
 
 /* Autotuner hook for the enumeration kernel (no reference counterpart):
  * carry-save blocks of 8 words per 64-word lane (0, 2, 5 or 8; -1 = built-in

@@ -3,6 +3,7 @@
  * Each function names the reference file:line range it restates. */
 #include "bmm_oracle.h"
 
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -1084,4 +1085,231 @@ done:
     free(offs);
     free(packed);
     return rc;
+}
+
+/* ---- SASelector (src/search/sa_selector*.cpp) ------------------------------ */
+typedef struct {
+    const uint64_t* words;
+    size_t stride, cols, W, n;
+    uint64_t tail;
+    int policy;
+    uint32_t* table;  /* pairwise: n x n synergy 2*popc(ri & rj) */
+    uint32_t* count;  /* higher order: per-column counts of the window */
+} orc_sa;
+
+static uint64_t sa_word(const orc_sa* S, size_t r, size_t w) {
+    const uint64_t v = S->words[r * S->stride + w];
+    return w + 1 == S->W ? (v & S->tail) : v;
+}
+
+static int64_t ho_term(uint32_t c) {
+    const int64_t n = (int64_t)c;
+    return n * (n - 1) * (n - 1);
+}
+
+static int64_t sa_score(orc_sa* S, const size_t* win, size_t t) {
+    int64_t s = 0;
+    if (S->policy == 0) {
+        for (size_t i = 0; i < t; ++i)
+            for (size_t j = i + 1; j < t; ++j)
+                s += (int64_t)S->table[win[i] * S->n + win[j]];
+        return s;
+    }
+    memset(S->count, 0, S->cols * sizeof(uint32_t));
+    for (size_t i = 0; i < t; ++i)
+        for (size_t w = 0; w < S->W; ++w)
+            for (uint64_t b = sa_word(S, win[i], w); b; b &= b - 1)
+                ++S->count[w * 64 + ctz64(b)];
+    for (size_t c = 0; c < S->cols; ++c)
+        s += ho_term(S->count[c]);
+    return s;
+}
+
+static int64_t sa_delta(const orc_sa* S, const size_t* win, size_t t, size_t out_idx, size_t in) {
+    const size_t out = win[out_idx];
+    int64_t d = 0;
+    if (S->policy == 0) {
+        for (size_t i = 0; i < t; ++i) {
+            if (i == out_idx)
+                continue;
+            d += (int64_t)S->table[in * S->n + win[i]];
+            d -= (int64_t)S->table[out * S->n + win[i]];
+        }
+        return d;
+    }
+    for (size_t w = 0; w < S->W; ++w) {
+        const uint64_t o = sa_word(S, out, w), a = sa_word(S, in, w);
+        for (uint64_t b = o & ~a; b; b &= b - 1) {
+            const uint32_t c = S->count[w * 64 + ctz64(b)];
+            d += ho_term(c - 1) - ho_term(c);
+        }
+        for (uint64_t b = a & ~o; b; b &= b - 1) {
+            const uint32_t c = S->count[w * 64 + ctz64(b)];
+            d += ho_term(c + 1) - ho_term(c);
+        }
+    }
+    return d;
+}
+
+static void sa_moved(orc_sa* S, size_t out, size_t in) {
+    if (S->policy == 0)
+        return;
+    for (size_t w = 0; w < S->W; ++w) {
+        const uint64_t o = sa_word(S, out, w), a = sa_word(S, in, w);
+        for (uint64_t b = o & ~a; b; b &= b - 1)
+            --S->count[w * 64 + ctz64(b)];
+        for (uint64_t b = a & ~o; b; b &= b - 1)
+            ++S->count[w * 64 + ctz64(b)];
+    }
+}
+
+static int cmp_size(const void* a, const void* b) {
+    const size_t x = *(const size_t*)a, y = *(const size_t*)b;
+    return x < y ? -1 : x > y;
+}
+
+/* lexicographic comparison of two sorted row lists of length t */
+static int rows_less(const size_t* a, const size_t* b, size_t t) {
+    for (size_t i = 0; i < t; ++i)
+        if (a[i] != b[i])
+            return a[i] < b[i];
+    return 0;
+}
+
+static int sa_better(int64_t ls, const size_t* lr, int64_t rs, const size_t* rr, size_t t) {
+    return ls != rs ? ls > rs : rows_less(lr, rr, t);
+}
+
+typedef struct {
+    int64_t score;
+    uint64_t accepted, iterations_run, best_iteration;
+} orc_sa_restart;
+
+static void sa_restart(orc_sa* S, size_t t, uint64_t iterations, uint64_t probe_samples,
+                       double p0, double cooling, double min_temp, uint64_t* rng,
+                       size_t* win, size_t* pool, size_t* tmp, size_t* best_rows,
+                       orc_sa_restart* best) {
+    const size_t n = S->n, np = n - t;
+    for (size_t i = 0; i < n; ++i)
+        pool[i] = i;
+    for (size_t i = 0; i < t; ++i) {
+        const size_t j = i + xs_index(rng, n - i);
+        const size_t x = pool[i];
+        pool[i] = pool[j];
+        pool[j] = x;
+    }
+    memcpy(win, pool, t * sizeof(size_t));
+    memmove(pool, pool + t, np * sizeof(size_t));
+    int64_t score = sa_score(S, win, t);
+    memcpy(best_rows, win, t * sizeof(size_t));
+    qsort(best_rows, t, sizeof(size_t), cmp_size);
+    best->score = score;
+    best->accepted = 0;
+    best->best_iteration = 0;
+    best->iterations_run = np == 0 ? 0 : iterations;
+    if (np == 0 || iterations == 0)
+        return;
+    double temp = 1.0;
+    {
+        const uint64_t samples = probe_samples > 1 ? probe_samples : 1;
+        double neg_sum = 0.0;
+        uint64_t neg = 0;
+        for (uint64_t k = 0; k < samples; ++k) {
+            const size_t iw = xs_index(rng, t);
+            const size_t ip = xs_index(rng, np);
+            const int64_t d = sa_delta(S, win, t, iw, pool[ip]);
+            if (d < 0) {
+                neg_sum += (double)(-d);
+                ++neg;
+            }
+        }
+        if (neg) {
+            const double avg = neg_sum / (double)neg;
+            const double t0 = -avg / log(p0);
+            temp = t0 < min_temp ? min_temp : t0;
+        }
+    }
+    uint64_t accepted = 0;
+    for (uint64_t it = 0; it < iterations; ++it) {
+        const size_t iw = xs_index(rng, t);
+        const size_t ip = xs_index(rng, np);
+        const size_t in = pool[ip];
+        const int64_t d = sa_delta(S, win, t, iw, in);
+        int accept = d > 0;
+        if (!accept && temp > min_temp)
+            accept = xs_unit(rng) < exp((double)d / temp);
+        if (accept) {
+            sa_moved(S, win[iw], in);
+            pool[ip] = win[iw];
+            win[iw] = in;
+            score += d;
+            ++accepted;
+            memcpy(tmp, win, t * sizeof(size_t));
+            qsort(tmp, t, sizeof(size_t), cmp_size);
+            if (sa_better(score, tmp, best->score, best_rows, t)) {
+                memcpy(best_rows, tmp, t * sizeof(size_t));
+                best->score = score;
+                best->accepted = accepted;
+                best->best_iteration = it + 1;
+            }
+        }
+        const double next = temp * cooling;
+        temp = min_temp < next ? next : min_temp;
+    }
+}
+
+long orc_sa_select(const uint64_t* words, size_t stride, size_t rows, size_t cols,
+                   size_t window_size, uint64_t iterations, uint64_t restarts, uint64_t seed,
+                   int score_policy, uint64_t probe_samples, double p0, double cooling,
+                   double min_temp, int64_t* scalars, size_t* out_rows) {
+    if (restarts == 0 || !(p0 > 0.0 && p0 < 1.0) || cooling <= 0.0 || cooling > 1.0 ||
+        min_temp <= 0.0 || window_size > rows)
+        return -1;
+    memset(scalars, 0, 6 * sizeof(int64_t));
+    uint64_t rng = orc_xs_seed(seed);
+    scalars[5] = (int64_t)rng;
+    if (window_size == 0)
+        return 0;
+    orc_sa S = {words, stride, cols, (cols + 63) / 64, rows, tail_mask_for_cols(cols),
+                score_policy, NULL, NULL};
+    if (score_policy == 0) {
+        S.table = (uint32_t*)calloc(rows * rows, sizeof(uint32_t));
+        for (size_t i = 0; i < rows; ++i)
+            for (size_t j = i + 1; j < rows; ++j) {
+                uint64_t ov = 0;
+                for (size_t w = 0; w < S.W; ++w)
+                    ov += popc64(sa_word(&S, i, w) & sa_word(&S, j, w));
+                S.table[i * rows + j] = S.table[j * rows + i] = (uint32_t)(2 * ov);
+            }
+    } else {
+        S.count = (uint32_t*)calloc(cols + 1, sizeof(uint32_t));
+    }
+    const size_t t = window_size;
+    size_t* win = (size_t*)malloc(t * sizeof(size_t));
+    size_t* pool = (size_t*)malloc(rows * sizeof(size_t));
+    size_t* tmp = (size_t*)malloc(t * sizeof(size_t));
+    size_t* cand = (size_t*)malloc(t * sizeof(size_t));
+    orc_sa_restart best, r;
+    int have = 0;
+    for (uint64_t k = 0; k < restarts; ++k) {
+        sa_restart(&S, t, iterations, probe_samples, p0, cooling, min_temp, &rng, win, pool, tmp,
+                   cand, &r);
+        if (!have || sa_better(r.score, cand, best.score, out_rows, t)) {
+            best = r;
+            memcpy(out_rows, cand, t * sizeof(size_t));
+            scalars[4] = (int64_t)k;
+            have = 1;
+        }
+    }
+    scalars[0] = best.score;
+    scalars[1] = (int64_t)best.accepted;
+    scalars[2] = (int64_t)best.iterations_run;
+    scalars[3] = (int64_t)best.best_iteration;
+    free(S.table);
+    free(S.count);
+    free(win);
+    free(pool);
+    free(tmp);
+    free(cand);
+    return (long)t;
 }

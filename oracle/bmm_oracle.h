@@ -136,6 +136,17 @@ long orc_exact_basis(const uint64_t* words, size_t stride, size_t cols, const si
 int orc_basis_weight_counts(const uint64_t* words, size_t stride, size_t cols, const size_t* win,
                             size_t t, uint64_t* counts);
 
+/* SASelector::select (src/search/sa_selector.cpp:10-75; restarts
+ * src/search/sa_selector_pairwise.cpp:118-170 and
+ * src/search/sa_selector_higher_order.cpp:171-225).  score_policy 0 pairwise,
+ * 1 higher order.  scalars[0..5] = score, accepted_moves, iterations_run,
+ * best_iteration, restart_index, seed; out_rows gets the sorted rows.
+ * Returns the row count, -1 for an invalid argument. */
+long orc_sa_select(const uint64_t* words, size_t stride, size_t rows, size_t cols,
+                   size_t window_size, uint64_t iterations, uint64_t restarts, uint64_t seed,
+                   int score_policy, uint64_t probe_samples, double p0, double cooling,
+                   double min_temp, int64_t* scalars, size_t* out_rows);
+
 #ifdef __cplusplus
 }
 #endif

@@ -107,6 +107,10 @@ def _load_port():
     lib.orc_exact_basis.restype = C.c_long
     lib.orc_exact_basis.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u32p, _u32p, _u64p]
     lib.orc_basis_weight_counts.argtypes = [_u64p, _sz, _sz, _szp, _sz, _u64p]
+    lib.orc_sa_select.restype = C.c_long
+    lib.orc_sa_select.argtypes = [_u64p, _sz, _sz, _sz, _sz, C.c_uint64, C.c_uint64, C.c_uint64,
+                                  C.c_int, C.c_uint64, C.c_double, C.c_double, C.c_double,
+                                  C.POINTER(C.c_int64), _szp]
     return lib
 
 
@@ -120,6 +124,28 @@ class _Searches:
 
     def _win(self, win):
         return np.ascontiguousarray(np.asarray(win, dtype=np.uintp))
+
+    def sa_select(self, m, cols, window_size, iterations=10000, restarts=8, seed=0,
+                  score_policy=0, temperature_probe_samples=64,
+                  initial_acceptance_probability=0.8, cooling_rate=0.99,
+                  min_temperature=1e-6):
+        """SASelector.select: dict of the SASelectionResult fields."""
+        m = np.ascontiguousarray(m, dtype=np.uint64)
+        sc = np.zeros(6, np.int64)
+        rows = np.zeros(max(window_size, 1), np.uintp)
+        args = (window_size, iterations, restarts, seed, score_policy, temperature_probe_samples,
+                initial_acceptance_probability, cooling_rate, min_temperature,
+                _ptr(sc, C.POINTER(C.c_int64)), _ptr(rows, _szp))
+        if self.prefix == "refh":
+            n = self.lib.refh_sa_select(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], *args)
+        else:
+            n = self.lib.orc_sa_select(_ptr(m, _u64p), m.shape[1], m.shape[0], cols, *args)
+        if n < 0:
+            raise ERRORS.get(n, OracleError)(f"checker error {n}")
+        return {"rows": [int(r) for r in rows[:n]], "score": int(sc[0]),
+                "accepted_moves": int(sc[1]), "iterations_run": int(sc[2]),
+                "best_iteration": int(sc[3]), "restart_index": int(sc[4]),
+                "seed": int(np.uint64(sc[5]))}
 
     def _result(self, count, masks, weights):
         if count < 0:
@@ -288,6 +314,8 @@ class Port(_Searches):
 class Ref(_Searches):
     """The reference library itself (oracle/_ref/libbmmref.so)."""
 
+    prefix = "refh"
+
     def __init__(self, lib):
         super().__init__(lib)
         L = lib
@@ -316,6 +344,10 @@ class Ref(_Searches):
         L.refh_exact_basis.restype = C.c_long
         L.refh_exact_basis.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, C.c_uint64, _sz,
                                        _u64p, _u32p, _u32p, _u64p, _u64p]
+        L.refh_sa_select.restype = C.c_long
+        L.refh_sa_select.argtypes = [_u64p, _sz, _sz, _sz, _sz, _sz, _sz, C.c_uint64, C.c_int,
+                                     _sz, C.c_double, C.c_double, C.c_double,
+                                     C.POINTER(C.c_int64), _szp]
         L.refh_island_run.restype = C.c_long
         L.refh_island_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_uint64,
                                       _sz, C.c_uint64, C.c_double, _u64p, C.POINTER(C.c_double)]

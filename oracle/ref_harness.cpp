@@ -25,6 +25,7 @@
 #include "bmmpy/search/bruteforce_search.hpp"
 #include "bmmpy/search/fwht_search.hpp"
 #include "bmmpy/search/mitm_fwht_search.hpp"
+#include "bmmpy/search/sa_selector.hpp"
 #include "bmmpy/search/split_window_prep.hpp"
 #include "bmmpy/solver/exact_basis_solver.hpp"
 
@@ -387,6 +388,39 @@ long refh_exact_basis(const std::uint64_t* words, std::size_t rows, std::size_t 
             for (std::size_t q = 0; q < stride; ++q)
                 basis_words[k * stride + q] = q < wpr ? r.basis_matrix.row_words(k)[q] : 0;
         return static_cast<long>(r.rank);
+    });
+}
+
+// SASelector(config).select(matrix, window_size).  scalars[0..5] = score,
+// accepted_moves, iterations_run, best_iteration, restart_index, seed;
+// out_rows gets the rows (room for window_size).  Returns the row count.
+long refh_sa_select(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                    std::size_t stride, std::size_t window_size, std::size_t iterations,
+                    std::size_t restarts, std::uint64_t seed, int score_policy,
+                    std::size_t probe_samples, double p0, double cooling, double min_temp,
+                    std::int64_t* scalars, std::size_t* out_rows) {
+    return guarded([&] {
+        auto m = make_matrix(words, rows, cols, stride);
+        bmmpy::SASelectorConfig c;
+        c.iterations = iterations;
+        c.restarts = restarts;
+        c.seed = seed;
+        c.score_policy = score_policy == 0 ? bmmpy::WindowScorePolicyKind::PairwiseSynergy
+                                           : bmmpy::WindowScorePolicyKind::HigherOrderSynergy;
+        c.temperature_probe_samples = probe_samples;
+        c.initial_acceptance_probability = p0;
+        c.cooling_rate = cooling;
+        c.min_temperature = min_temp;
+        const bmmpy::SASelectionResult r = bmmpy::SASelector(c).select(m, window_size);
+        scalars[0] = r.score;
+        scalars[1] = static_cast<std::int64_t>(r.accepted_moves);
+        scalars[2] = static_cast<std::int64_t>(r.iterations_run);
+        scalars[3] = static_cast<std::int64_t>(r.best_iteration);
+        scalars[4] = static_cast<std::int64_t>(r.restart_index);
+        scalars[5] = static_cast<std::int64_t>(r.seed);
+        for (std::size_t i = 0; i < r.rows.size(); ++i)
+            out_rows[i] = r.rows[i];
+        return static_cast<long>(r.rows.size());
     });
 }
 
