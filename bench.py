@@ -35,6 +35,10 @@ resident rows, ``e2e`` from the public solve() on host windows.
 the planted 512 x 65536 matrix: ``value`` from the device synergy table,
 ``e2e`` from select().
 
+``--workload io`` (1 GPU) measures matrix IO on the same matrix: the text
+payload parsed on the device, BitMatrix.from_text and a binary file loaded
+into device memory end to end.
+
 ``--workload ga`` (1 GPU) measures the island-model GA instead: the planted
 256 x 8192 matrix (density 0.01, 5000 scrambles, seed 7), 64 islands x 256,
 ring migration every 20 generations, stop at the planted weight or the
@@ -700,6 +704,120 @@ def run_sa(args):
     return 0
 
 
+def run_io(args):
+    """Matrix IO on the planted 512 x 65536 matrix: text payload parsed on the
+    device from resident bytes (value, GB/s of text), and end to end through
+    the public API: BitMatrix.from_text on host text, and a BMMPYB1 file
+    loaded straight into device memory."""
+    import tempfile
+
+    import torch
+
+    import bmmpy_b200 as bmm
+    from bmmpy_b200 import _native as N
+    from oracle.oracle import port, ref
+
+    words, _ = port().gen_instance(C3["rows"], C3["cols"], C3["p"], C3["seed"], C3["scrambles"])
+    m = bmm.BitMatrix(C3["rows"], C3["cols"])
+    m.words[:] = words[:, : m.stride_words]
+    text = m.to_text().encode()
+    head = len(f"{m.rows} {m.cols}")
+    if args.impl == "reference":
+        R = ref()
+        t0 = time.perf_counter()
+        for _ in range(max(1, args.steps)):
+            R.matrix_from_text(text)
+        dt = (time.perf_counter() - t0) / max(1, args.steps)
+        v = len(text) / dt / 1e9
+        print(json.dumps({"impl": "reference", "metric": "text matrix parse GB/s", "value": v,
+                          "unit": "GB/s", "higher_is_better": True, "n_gpus": 0,
+                          "config": {"workload": "BitMatrix::load_text of the planted 512x65536 "
+                                                 "matrix (33.5 MB of text)"},
+                          "cpu_baseline": {"value": v, "unit": "GB/s", "cores": 1,
+                                           "kind": "reference", "sample": "whole matrix"},
+                          "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    payload = torch.from_numpy(np.frombuffer(text[head:], dtype=np.uint8).copy()).to(dev)
+    d_words = torch.empty(m.rows * m.stride_words, dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    L = N.lib()
+
+    def launch():
+        N.check(L.bmm_matrix_from_text_dev(payload.data_ptr(), payload.numel(),
+                                           d_words.data_ptr(), m.stride_words, m.rows, m.cols,
+                                           stream.cuda_stream))
+
+    for _ in range(args.warmup):
+        launch()
+    sampler = clock_sampler(None)
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        launch()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    time.sleep(0.3)  # the timed region is shorter than one clock sample
+    clocks = clock_summary(sampler)
+    ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+    got = d_words.cpu().numpy().view(np.uint64).reshape(m.rows, m.stride_words)
+    assert np.array_equal(got, m.words)
+    algo = payload.numel() + m.words.nbytes  # text read once, rows written once
+    peak = 6650.0
+    e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        back = bmm.BitMatrix.from_text(text)
+    e_dt = (time.perf_counter() - t0) / e_steps
+    assert back == m
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "m.bin")
+        m.save_binary_file(path)
+        bin_bytes = os.path.getsize(path)
+        t0 = time.perf_counter()
+        for _ in range(e_steps):
+            N.check(L.bmm_matrix_load_binary_dev(path.encode(), d_words.data_ptr(),
+                                                 m.stride_words, m.rows, m.cols,
+                                                 stream.cuda_stream))
+        b_dt = (time.perf_counter() - t0) / e_steps
+    line = {
+        "metric": "text matrix parse GB/s", "value": payload.numel() / (ms / 1e3) / 1e9,
+        "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic planted matrix (xorshift64 seed 2)",
+        "config": {"workload": "text payload of the planted 512x65536 matrix (33.5 MB) parsed "
+                               "on the device; BMMPYB1 file (4 MB) loaded into device memory",
+                   "l2": "flushed before every timed step (256 MB device write)"},
+        "e2e": {"value": len(text) / e_dt / 1e9, "unit": "GB/s",
+                "h2d_bytes_per_step": len(text), "d2h_bytes_per_step": int(m.words.nbytes),
+                "seconds_per_parse": e_dt, "binary_file_to_device_s": b_dt,
+                "binary_file_bytes": bin_bytes},
+        "gpu_launches": 3 * args.steps,
+        "roofline": {"bound": "hbm", "achieved": algo / (ms / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": algo / (ms / 1e3) / 1e9 / peak,
+                     "peak_source": "fallback 6.65 TB/s (no measured peaks file)",
+                     "traffic": None},
+        "clocks": clocks,
+    }
+    if not args.no_cpu_baseline:
+        R = ref()
+        if R is not None:
+            t0 = time.perf_counter()
+            R.matrix_from_text(text)
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": len(text) / dt / 1e9, "unit": "GB/s", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": "BitMatrix::load_text of the same 33.5 MB text"}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -708,7 +826,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa"])
+    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa", "io"])
     ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
     ap.add_argument("--seeds", type=int, default=2, help="GA: seeds per variant")
     ap.add_argument("--islands", type=int, default=64)
@@ -723,6 +841,8 @@ def main():
         return run_basis(args)
     if args.workload == "sa":
         return run_sa(args)
+    if args.workload == "io":
+        return run_io(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

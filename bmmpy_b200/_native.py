@@ -16,7 +16,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libbmm_b200.so")
 
-OK, EINVAL, EOVERFLOW, ECUDA, ENODEV, ETIMEOUT, ENOMEM, ERUNTIME = 0, -1, -2, -3, -4, -5, -6, -7
+OK, EINVAL, EOVERFLOW, ECUDA, ENODEV, ETIMEOUT, ENOMEM, ERUNTIME, EMATRIX = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8)
 
 
 class Candidate_t(C.Structure):
@@ -185,6 +186,16 @@ SIGNATURES = {
     "bmm_sa_select": [_u64p, _sz, _sz, _sz, _sz, C.POINTER(SaConfig_t), C.POINTER(SaResult_t),
                       _szp],
     "bmm_sa_pairwise_table": [_u64p, _sz, _sz, _sz, _u32p],
+    "bmm_matrix_text_header": [C.c_char_p, _sz, _u64p, _u64p],
+    "bmm_matrix_from_text": [C.c_char_p, _sz, _u64p, _sz, _sz, _sz],
+    "bmm_matrix_from_text_dev": [_vp, _sz, _vp, _sz, _sz, _sz, _vp],
+    "bmm_matrix_text_size": [_sz, _sz, _szp],
+    "bmm_matrix_to_text": [_u64p, _sz, _sz, _sz, C.c_char_p, _sz, _szp],
+    "bmm_matrix_save_binary": [C.c_char_p, _u64p, _sz, _sz, _sz],
+    "bmm_matrix_binary_header": [C.c_char_p, _u64p, _u64p],
+    "bmm_matrix_load_binary": [C.c_char_p, _u64p, _sz, _sz, _sz],
+    "bmm_matrix_load_binary_dev": [C.c_char_p, _vp, _sz, _sz, _sz, _vp],
+    "bmm_matrix_hash": [_u64p, _sz, _sz, _sz, C.c_char_p],
     "bmm_sa_pairwise_table_dev": [_vp, _sz, _sz, _sz, _vp, _vp],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,
@@ -229,6 +240,12 @@ def check(rc: int, what: str = "") -> None:
         raise OverflowError(msg)
     if rc == ENOMEM:
         raise MemoryError(msg)
+    if rc == EMATRIX:
+        from .matrix import MatrixError
+
+        raise MatrixError(msg)
+    if rc == ERUNTIME:
+        raise RuntimeError(msg)
     raise RuntimeError(f"{msg} (status {rc})")
 
 

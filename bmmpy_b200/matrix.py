@@ -7,6 +7,10 @@ in word c // 64 at bit c % 64, row stride padded to a multiple of 4 words
 in a numpy array (host memory) that the search entry points hand to the
 device library.
 
+Text and binary IO and ``hash()`` follow src/core/bit_matrix_io.cpp and
+src/core/bit_matrix_hash.cpp (formats, messages); text is parsed and
+formatted on the device.
+
 ``RowWindow`` mirrors bmmpy.RowWindow (include/bmmpy/core/row_window.hpp):
 an ordered list of unique rows of one matrix; it borrows the matrix, so
 applying a candidate through the window changes the matrix.
@@ -14,6 +18,8 @@ applying a candidate through the window changes the matrix.
 
 from __future__ import annotations
 
+import ctypes as C
+import os
 from collections.abc import Sequence
 
 import numpy as np
@@ -228,12 +234,83 @@ class BitMatrix:
             self._words[r] = source._words[i]
 
     def to_rows(self) -> list[str]:
+        if self._rows == 0 or self._cols == 0:
+            return [""] * self._rows
         bits = np.unpackbits(self._words.view(np.uint8).reshape(self._rows, -1), axis=1,
                              bitorder="little")
         return ["".join("1" if b else "0" for b in row[: self._cols]) for row in bits]
 
+    # -- text / binary IO and hash (src/core/bit_matrix_io.cpp,
+    #    src/core/bit_matrix_hash.cpp; formatted and parsed on the device) --------
     def to_text(self) -> str:
-        return "\n".join(self.to_rows())
+        """save_text: "rows cols\\n" then one '0'/'1' line per row."""
+        from . import _native as N
+
+        n = C.c_size_t(0)
+        N.check(N.lib().bmm_matrix_text_size(self._rows, self._cols, C.byref(n)))
+        buf = C.create_string_buffer(max(1, n.value))
+        N.check(N.lib().bmm_matrix_to_text(N.u64p(self._words), self.stride_words, self._rows,
+                                           self._cols, buf, n.value, None))
+        return buf.raw[: n.value].decode("ascii")
+
+    __str__ = to_text
+
+    @classmethod
+    def from_text(cls, text) -> "BitMatrix":
+        """load_text over a string: whitespace between bits is ignored."""
+        from . import _native as N
+
+        data = text.encode("ascii", "replace") if isinstance(text, str) else bytes(text)
+        rows, cols = C.c_uint64(0), C.c_uint64(0)
+        N.check(N.lib().bmm_matrix_text_header(data, len(data), C.byref(rows), C.byref(cols)))
+        m = cls(rows.value, cols.value)
+        N.check(N.lib().bmm_matrix_from_text(data, len(data), N.u64p(m._words), m.stride_words,
+                                             m._rows, m._cols))
+        return m
+
+    @classmethod
+    def load_text_file(cls, path) -> "BitMatrix":
+        try:
+            with open(os.fspath(path), "rb") as f:
+                data = f.read()
+        except OSError:
+            raise RuntimeError("failed to open matrix text file for reading") from None
+        return cls.from_text(data)
+
+    def save_text_file(self, path) -> None:
+        text = self.to_text()
+        try:
+            with open(os.fspath(path), "w", newline="") as f:
+                f.write(text)
+        except OSError:
+            raise RuntimeError("failed to open matrix text file for writing") from None
+
+    def save_binary_file(self, path) -> None:
+        from . import _native as N
+
+        N.check(N.lib().bmm_matrix_save_binary(os.fsencode(path), N.u64p(self._words),
+                                               self.stride_words, self._rows, self._cols))
+
+    @classmethod
+    def load_binary_file(cls, path) -> "BitMatrix":
+        from . import _native as N
+
+        p = os.fsencode(path)
+        rows, cols = C.c_uint64(0), C.c_uint64(0)
+        N.check(N.lib().bmm_matrix_binary_header(p, C.byref(rows), C.byref(cols)))
+        m = cls(rows.value, cols.value)
+        N.check(N.lib().bmm_matrix_load_binary(p, N.u64p(m._words), m.stride_words, m._rows,
+                                               m._cols))
+        return m
+
+    def hash(self) -> str:
+        """SHA-256 hex of rows, cols and the row words (bits past cols cleared)."""
+        from . import _native as N
+
+        out = C.create_string_buffer(65)
+        N.check(N.lib().bmm_matrix_hash(N.u64p(self._words), self.stride_words, self._rows,
+                                        self._cols, out))
+        return out.value.decode("ascii")
 
     def __eq__(self, other) -> bool:
         return (isinstance(other, BitMatrix) and self.shape == other.shape

@@ -27,6 +27,9 @@
  *   bmm_sa_select        SASelector::select  src/search/sa_selector.cpp:10-75,
  *                        src/search/sa_selector_pairwise.cpp:21-172,
  *                        src/search/sa_selector_higher_order.cpp:11-227.
+ *   bmm_matrix_*         BitMatrix text / binary IO and hash
+ *                        src/core/bit_matrix_io.cpp:34-175,
+ *                        src/core/bit_matrix_hash.cpp:30-58.
  *   bmm_exact_basis      ExactBasisSolver::solve
  *                        src/solver/exact_basis_solver.cpp:58-157,
  *                        include/bmmpy/solver/exact_basis_solver.hpp:12-43.
@@ -36,7 +39,8 @@
  *    and never throws; bmm_last_error() gives the calling thread's message.
  *    The status classes map to the reference's exception types:
  *    BMM_EINVAL -> std::invalid_argument, BMM_EOVERFLOW -> std::overflow_error,
- *    BMM_ECUDA / BMM_ENODEV / BMM_ETIMEOUT / BMM_ERUNTIME -> std::runtime_error.
+ *    BMM_ECUDA / BMM_ENODEV / BMM_ETIMEOUT / BMM_ERUNTIME -> std::runtime_error,
+ *    BMM_EMATRIX -> bmmpy::MatrixError (a std::runtime_error).
  *  - A matrix is row-major packed uint64 words: bit c of a row sits in word
  *    c >> 6 at bit c & 63; `stride` words separate rows; bits at and past
  *    `cols` must be zero (the reference BitMatrix layout).  A window is a list
@@ -75,6 +79,7 @@ extern "C" {
 #define BMM_ETIMEOUT (-5)
 #define BMM_ENOMEM (-6)
 #define BMM_ERUNTIME (-7)
+#define BMM_EMATRIX (-8)
 
 /* DeviceTopKEntry of include/bmmpy/search/cuda_launch_topk.cuh:11-14 (16 B). */
 typedef struct bmm_candidate {
@@ -461,6 +466,45 @@ BMM_API int bmm_sa_pairwise_table(const uint64_t* words, size_t stride, size_t r
                                   uint32_t* table);
 BMM_API int bmm_sa_pairwise_table_dev(const uint64_t* words, size_t stride, size_t rows,
                                       size_t cols, uint32_t* table, void* stream);
+
+/* ---- matrix IO (src/core/bit_matrix_io.cpp, bit_matrix_hash.cpp) ----------
+ * Text: "rows cols\n", then rows x cols '0'/'1' characters; on input any ASCII
+ * whitespace may separate them (BitMatrix::load_text / save_text).  Binary:
+ * "BMMPYB1\0", u64 rows, u64 cols (little endian), then (cols + 63) / 64
+ * words per row, unpadded (load_binary / save_binary).  Errors carry the
+ * reference's messages: BMM_ERUNTIME for its std::runtime_error, BMM_EMATRIX
+ * for MatrixError (SizeTooLarge). */
+
+/* The dimensions of a text matrix (in >> rows >> cols). */
+BMM_API int bmm_matrix_text_header(const char* text, size_t len, uint64_t* rows, uint64_t* cols);
+/* Parse a whole text matrix (header included) into rows x stride words; the
+ * payload is parsed on the device. */
+BMM_API int bmm_matrix_from_text(const char* text, size_t len, uint64_t* words, size_t stride,
+                                 size_t rows, size_t cols);
+/* Device form: `payload` is the text after the two header numbers (rows and
+ * cols from bmm_matrix_text_header), already on the device; words (rows x
+ * stride, device) are overwritten on `stream`, which is synchronised to
+ * report the parse result. */
+BMM_API int bmm_matrix_from_text_dev(const char* payload, size_t len, uint64_t* words,
+                                     size_t stride, size_t rows, size_t cols, void* stream);
+/* Bytes of save_text's output for a rows x cols matrix. */
+BMM_API int bmm_matrix_text_size(size_t rows, size_t cols, size_t* len);
+/* save_text into out (cap bytes, not NUL-terminated); formatted on the device. */
+BMM_API int bmm_matrix_to_text(const uint64_t* words, size_t stride, size_t rows, size_t cols,
+                               char* out, size_t cap, size_t* len);
+BMM_API int bmm_matrix_save_binary(const char* path, const uint64_t* words, size_t stride,
+                                   size_t rows, size_t cols);
+BMM_API int bmm_matrix_binary_header(const char* path, uint64_t* rows, uint64_t* cols);
+/* Load into host words (rows x stride, padding words cleared) ... */
+BMM_API int bmm_matrix_load_binary(const char* path, uint64_t* words, size_t stride, size_t rows,
+                                   size_t cols);
+/* ... or straight into device words through pinned staging (synchronous). */
+BMM_API int bmm_matrix_load_binary_dev(const char* path, uint64_t* words, size_t stride,
+                                       size_t rows, size_t cols, void* stream);
+/* BitMatrix::hash: SHA-256 hex (64 characters + NUL) of rows, cols and the
+ * tail-masked row words as little-endian u64 values. */
+BMM_API int bmm_matrix_hash(const uint64_t* words, size_t stride, size_t rows, size_t cols,
+                            char* hex);
 
 /* Autotuner hook for the enumeration kernel (no reference counterpart):
  * carry-save blocks of 8 words per 64-word lane (0, 2, 5 or 8; -1 = built-in

@@ -39,6 +39,79 @@ class OracleError(RuntimeError):
     pass
 
 
+class MatrixErrorRef(RuntimeError):
+    """The reference's MatrixError, as raised through the harness."""
+
+
+# ---- matrix IO restated (src/core/bit_matrix_io.cpp:34-175,
+#      src/core/bit_matrix_hash.cpp:30-58); plain Python for small matrices ----
+_WS = b" \n\r\t\f\v"
+
+
+def text_format(words, rows, cols) -> bytes:
+    """save_text: header line, then one '0'/'1' line per row."""
+    out = [f"{rows} {cols}\n".encode()]
+    for r in range(rows):
+        line = bytearray(b"0" * cols)
+        for c in range(cols):
+            if (int(words[r][c // 64]) >> (c % 64)) & 1:
+                line[c] = ord("1")
+        out.append(bytes(line) + b"\n")
+    return b"".join(out)
+
+
+def text_parse(text: bytes):
+    """load_text: (rows, cols, list of row bit lists) or raises RuntimeError
+    with the reference's message."""
+    p, n, dims = 0, len(text), []
+    for _ in range(2):
+        while p < n and text[p:p + 1] in [bytes([b]) for b in _WS]:
+            p += 1
+        neg = False
+        if p < n and text[p:p + 1] in (b"+", b"-"):
+            neg = text[p:p + 1] == b"-"
+            p += 1
+        q = p
+        while p < n and 48 <= text[p] <= 57:
+            p += 1
+        if q == p or int(text[q:p]) >= 1 << 64:
+            raise RuntimeError("failed to read matrix text header")
+        v = int(text[q:p])
+        dims.append((-v) % (1 << 64) if neg else v)
+    rows, cols = dims
+    total = rows * cols
+    bits = []
+    while len(bits) < total and p < n:
+        ch = text[p]
+        p += 1
+        if ch in (48, 49):
+            bits.append(ch - 48)
+        elif ch not in _WS:
+            raise RuntimeError("matrix text contains invalid character")
+    if len(bits) != total:
+        raise RuntimeError("failed to read matrix text payload")
+    while p < n:
+        if text[p] not in _WS:
+            raise RuntimeError("matrix text contains trailing data")
+        p += 1
+    return rows, cols, [bits[r * cols:(r + 1) * cols] for r in range(rows)]
+
+
+def matrix_hash(words, rows, cols) -> str:
+    """SHA-256 (hashlib) over little-endian u64 rows, cols, tail-masked words."""
+    import hashlib
+
+    h = hashlib.sha256()
+    h.update(int(rows).to_bytes(8, "little") + int(cols).to_bytes(8, "little"))
+    W = (cols + 63) // 64
+    tail = (1 << (cols % 64)) - 1 if cols % 64 else (1 << 64) - 1
+    for r in range(rows):
+        for w in range(W):
+            v = int(words[r][w]) & (tail if w == W - 1 else (1 << 64) - 1)
+            h.update(v.to_bytes(8, "little"))
+    return h.hexdigest()
+
+
 class GaConfig(C.Structure):
     """GeneticAlgorithmConfig as orc_ga_config / refh_ga_config (flags: 1
     max_generations, 2 max_stale_generations, 4 target_total_weight)."""
@@ -348,6 +421,18 @@ class Ref(_Searches):
         L.refh_sa_select.argtypes = [_u64p, _sz, _sz, _sz, _sz, _sz, _sz, C.c_uint64, C.c_int,
                                      _sz, C.c_double, C.c_double, C.c_double,
                                      C.POINTER(C.c_int64), _szp]
+        L.refh_last_error.restype = C.c_char_p
+        L.refh_last_error.argtypes = []
+        L.refh_matrix_from_text.restype = C.c_long
+        L.refh_matrix_from_text.argtypes = [C.c_char_p, _sz, _u64p, _u64p, _sz, _sz]
+        L.refh_matrix_to_text.restype = C.c_long
+        L.refh_matrix_to_text.argtypes = [_u64p, _sz, _sz, _sz, C.c_char_p, _sz]
+        L.refh_matrix_hash.restype = C.c_long
+        L.refh_matrix_hash.argtypes = [_u64p, _sz, _sz, _sz, C.c_char_p]
+        L.refh_matrix_save_binary.restype = C.c_long
+        L.refh_matrix_save_binary.argtypes = [C.c_char_p, _u64p, _sz, _sz, _sz]
+        L.refh_matrix_load_binary.restype = C.c_long
+        L.refh_matrix_load_binary.argtypes = [C.c_char_p, _u64p, _u64p, _sz, _sz]
         L.refh_island_run.restype = C.c_long
         L.refh_island_run.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _sz, C.c_uint64,
                                       _sz, C.c_uint64, C.c_double, _u64p, C.POINTER(C.c_double)]
@@ -469,6 +554,60 @@ class Ref(_Searches):
                 "basis_masks": [int(x) for x in masks[:r]],
                 "basis_weights": [int(x) for x in ws[:r]],
                 "transform": [int(x) for x in tr[:r]], "basis_words": bw[:r].copy()}
+
+    def _raise(self, rc):
+        msg = self.lib.refh_last_error().decode()
+        raise {-5: RuntimeError, -6: MatrixErrorRef}.get(rc, ERRORS.get(rc, OracleError))(msg)
+
+    def matrix_from_text(self, text: bytes):
+        """BitMatrix::load_text: (words (rows, stride), rows, cols); raises with
+        the reference's message (RuntimeError, or MatrixErrorRef)."""
+        dims = np.zeros(2, np.uint64)
+        rc = self.lib.refh_matrix_from_text(text, len(text), _ptr(dims, _u64p),
+                                            _ptr(np.zeros(1, np.uint64), _u64p), 1, 0)
+        if rc < 0:
+            self._raise(rc)
+        rows, cols = int(dims[0]), int(dims[1])
+        stride = max(4, ((cols + 63) // 64 + 3) // 4 * 4)
+        out = np.zeros((max(rows, 1), stride), np.uint64)
+        rc = self.lib.refh_matrix_from_text(text, len(text), _ptr(dims, _u64p), _ptr(out, _u64p),
+                                            stride, out.size)
+        return out[:rows], rows, cols
+
+    def matrix_to_text(self, m, cols) -> bytes:
+        m = np.ascontiguousarray(m, dtype=np.uint64)
+        n = self.lib.refh_matrix_to_text(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], None, 0)
+        buf = C.create_string_buffer(max(n, 1))
+        self.lib.refh_matrix_to_text(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], buf, n)
+        return buf.raw[:n]
+
+    def matrix_hash(self, m, cols) -> str:
+        m = np.ascontiguousarray(m, dtype=np.uint64)
+        out = C.create_string_buffer(65)
+        rc = self.lib.refh_matrix_hash(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], out)
+        if rc < 0:
+            self._raise(rc)
+        return out.value.decode()
+
+    def matrix_save_binary(self, path, m, cols):
+        m = np.ascontiguousarray(m, dtype=np.uint64)
+        rc = self.lib.refh_matrix_save_binary(os.fsencode(path), _ptr(m, _u64p), m.shape[0], cols,
+                                              m.shape[1])
+        if rc < 0:
+            self._raise(rc)
+
+    def matrix_load_binary(self, path):
+        p = os.fsencode(path)
+        dims = np.zeros(2, np.uint64)
+        rc = self.lib.refh_matrix_load_binary(p, _ptr(dims, _u64p),
+                                              _ptr(np.zeros(1, np.uint64), _u64p), 1, 0)
+        if rc < 0:
+            self._raise(rc)
+        rows, cols = int(dims[0]), int(dims[1])
+        stride = max(4, ((cols + 63) // 64 + 3) // 4 * 4)
+        out = np.zeros((max(rows, 1), stride), np.uint64)
+        self.lib.refh_matrix_load_binary(p, _ptr(dims, _u64p), _ptr(out, _u64p), stride, out.size)
+        return out[:rows], rows, cols
 
     def island_run(self, m, cols, win, islands, population, interval, seed, max_gens, target,
                    cap_seconds):

@@ -30,6 +30,8 @@
 #include "bmmpy/solver/exact_basis_solver.hpp"
 
 #include <chrono>
+#include <sstream>
+#include <string>
 #include <cstdint>
 #include <cstring>
 #include <memory>
@@ -55,20 +57,38 @@ bmmpy::BitMatrix make_matrix(const std::uint64_t* words, std::size_t rows, std::
     return m;
 }
 
+thread_local std::string g_last_error;
+
 template <typename Fn> long guarded(Fn&& fn) {
     try {
+        g_last_error.clear();
         return fn();
-    } catch (const std::invalid_argument&) {
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
         return -1;
-    } catch (const std::overflow_error&) {
+    } catch (const std::overflow_error& e) {
+        g_last_error = e.what();
         return -2;
-    } catch (const std::out_of_range&) {
+    } catch (const std::out_of_range& e) {
+        g_last_error = e.what();
         return -3;
-    } catch (const std::logic_error&) {
+    } catch (const std::logic_error& e) {
+        g_last_error = e.what();
         return -4;
-    } catch (const std::exception&) {
+    } catch (const bmmpy::MatrixError& e) {
+        g_last_error = e.what();
+        return -6;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
         return -5;
     }
+}
+
+void copy_words(const bmmpy::BitMatrix& m, std::uint64_t* out, std::size_t stride) {
+    const std::size_t wpr = m.words_per_row();
+    for (std::size_t r = 0; r < m.rows(); ++r)
+        for (std::size_t q = 0; q < stride; ++q)
+            out[r * stride + q] = q < wpr ? m.row_words(r)[q] : 0;
 }
 
 long emit(const std::vector<bmmpy::Candidate>& cands, std::size_t cap, std::uint64_t* out_mask,
@@ -421,6 +441,69 @@ long refh_sa_select(const std::uint64_t* words, std::size_t rows, std::size_t co
         for (std::size_t i = 0; i < r.rows.size(); ++i)
             out_rows[i] = r.rows[i];
         return static_cast<long>(r.rows.size());
+    });
+}
+
+// Message of the last exception a shim caught on this thread.
+const char* refh_last_error() { return g_last_error.c_str(); }
+
+// BitMatrix::load_text over a string.  dims[0..1] = rows, cols; the words go
+// to out (rows x stride) when cap_words allows.  Returns 0.
+long refh_matrix_from_text(const char* text, std::size_t len, std::uint64_t* dims,
+                           std::uint64_t* out, std::size_t stride, std::size_t cap_words) {
+    return guarded([&] {
+        std::istringstream in(std::string(text, len));
+        const bmmpy::BitMatrix m = bmmpy::BitMatrix::load_text(in);
+        dims[0] = m.rows();
+        dims[1] = m.cols();
+        if (m.rows() * stride <= cap_words)
+            copy_words(m, out, stride);
+        return 0L;
+    });
+}
+
+// BitMatrix::save_text; returns the length (the text goes to out when it fits).
+long refh_matrix_to_text(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                         std::size_t stride, char* out, std::size_t cap) {
+    return guarded([&] {
+        auto m = make_matrix(words, rows, cols, stride);
+        std::ostringstream o;
+        m.save_text(o);
+        const std::string t = o.str();
+        if (t.size() <= cap)
+            std::memcpy(out, t.data(), t.size());
+        return static_cast<long>(t.size());
+    });
+}
+
+// BitMatrix::hash into hex (65 bytes).
+long refh_matrix_hash(const std::uint64_t* words, std::size_t rows, std::size_t cols,
+                      std::size_t stride, char* hex) {
+    return guarded([&] {
+        const std::string h = make_matrix(words, rows, cols, stride).hash();
+        std::memcpy(hex, h.c_str(), h.size() + 1);
+        return 0L;
+    });
+}
+
+long refh_matrix_save_binary(const char* path, const std::uint64_t* words, std::size_t rows,
+                             std::size_t cols, std::size_t stride) {
+    return guarded([&] {
+        make_matrix(words, rows, cols, stride).save_binary(std::filesystem::path(path));
+        return 0L;
+    });
+}
+
+// BitMatrix::load_binary: dims and words as refh_matrix_from_text.
+long refh_matrix_load_binary(const char* path, std::uint64_t* dims, std::uint64_t* out,
+                             std::size_t stride, std::size_t cap_words) {
+    return guarded([&] {
+        const bmmpy::BitMatrix m = bmmpy::BitMatrix::load_binary(std::filesystem::path(path));
+        dims[0] = m.rows();
+        dims[1] = m.cols();
+        if (m.rows() * stride <= cap_words)
+            copy_words(m, out, stride);
+        return 0L;
     });
 }
 
