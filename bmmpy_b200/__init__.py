@@ -36,7 +36,7 @@ from .search import (
     SASelector,
 )
 
-from .workflows import search_apply
+from .workflows import DeviceMatrix, search_apply
 
 __all__ = [
     "ApplyResult",
@@ -70,4 +70,5 @@ __all__ = [
     "matrix_from_rows",
     "solver",
     "search_apply",
+    "DeviceMatrix",
 ]

@@ -131,6 +131,20 @@ class SaResult_t(C.Structure):
                 ("restart_index", C.c_uint64), ("seed", C.c_uint64), ("n_rows", C.c_size_t)]
 
 
+class SweepConfig_t(C.Structure):
+    """bmm_sweep_config."""
+
+    _fields_ = [("max_candidates", C.c_uint64), ("applier", C.c_uint32),
+                ("stochastic", C.c_uint32), ("min_gain", C.c_uint64), ("seed", C.c_uint64),
+                ("require_improvement", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class ApplyResult_t(C.Structure):
+    """bmm_apply_result."""
+
+    _fields_ = [("applied_count", C.c_uint64), ("weight_improvement", C.c_uint64)]
+
+
 # name -> argtypes (all return int unless listed in _RESTYPES)
 SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
@@ -196,6 +210,8 @@ SIGNATURES = {
     "bmm_matrix_load_binary": [C.c_char_p, _u64p, _sz, _sz, _sz],
     "bmm_matrix_load_binary_dev": [C.c_char_p, _vp, _sz, _sz, _sz, _vp],
     "bmm_matrix_hash": [_u64p, _sz, _sz, _sz, C.c_char_p],
+    "bmm_search_apply_dev": [_vp, _sz, _sz, _u32p, _sz, _sz, C.POINTER(SweepConfig_t),
+                             C.POINTER(ApplyResult_t), _u64p, _vp],
     "bmm_sa_pairwise_table_dev": [_vp, _sz, _sz, _sz, _vp, _vp],
 }
 _RESTYPES = {"bmm_last_error": C.c_char_p, "bmm_version": C.c_char_p,

@@ -47,6 +47,10 @@ enum Slot : int {
     kSlotExtra0,
     kSlotExtra1,
     kSlotSlices,
+    kSlotSweepWin,    // search -> apply sweeps: window lists, new rows, states, order
+    kSlotSweepNew,
+    kSlotSweepState,
+    kSlotSweepOrder,
     kSlotCount
 };
 

@@ -506,6 +506,37 @@ BMM_API int bmm_matrix_load_binary_dev(const char* path, uint64_t* words, size_t
 BMM_API int bmm_matrix_hash(const uint64_t* words, size_t stride, size_t rows, size_t cols,
                             char* hex);
 
+/* ---- device-resident search -> apply ---------------------------------------
+ * search_apply (bmmpy/workflows.py:45-90) over n_windows windows of t rows of
+ * a DEVICE matrix, in order, all on `stream`: per window the exact top-k
+ * spectrum search (MitmFwhtSearch / FwhtSearch candidates) and the applier
+ * (0: GreedyApplier(min_gain, stochastic, seed) -- one generator carried from
+ * window to window as one applier object would; 1: GlobalGreedyApplier(
+ * require_improvement)) update the matrix rows in place.  windows: host array
+ * of n_windows x t row indices.  results: one ApplyResult per window.
+ * cfg->seed is the greedy generator's state on entry (0 -> 0xDEADB, as the
+ * constructor); final_state (optional) receives it on exit.  Synchronises
+ * `stream` once, at the end. */
+typedef struct bmm_sweep_config {
+    uint64_t max_candidates;
+    uint32_t applier;
+    uint32_t stochastic;
+    uint64_t min_gain;
+    uint64_t seed;
+    uint32_t require_improvement;
+    uint32_t reserved;
+} bmm_sweep_config;
+
+typedef struct bmm_apply_result {
+    uint64_t applied_count;
+    uint64_t weight_improvement;
+} bmm_apply_result;
+
+BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
+                                 const uint32_t* windows, size_t t, size_t n_windows,
+                                 const bmm_sweep_config* cfg, bmm_apply_result* results,
+                                 uint64_t* final_state, void* stream);
+
 /* Autotuner hook for the enumeration kernel (no reference counterpart):
  * carry-save blocks of 8 words per 64-word lane (0, 2, 5 or 8; -1 = built-in
  * policy).  Process-wide; results never change, only speed. */
