@@ -13,8 +13,11 @@
 // GEMM kernel.  C[M x N] = A[M x K] . B[N x K]^T for any element strides of A
 // and B (transposes are folded into the staging loads), FP32 or BF16 sources
 // rounded to BF16 while they are written to shared memory in the canonical
-// K-major layout; one CTA per 128 x 256 output tile, K in chunks of 64 (four
-// K=16 MMAs per chunk), TMEM accumulator of 256 columns; the epilogue reads
+// K-major layout (as 16-byte vectors where the strides allow: K-contiguous
+// rows directly, row-contiguous operands through 8 x 8 register transposes);
+// one CTA per 128 x 256 output tile, K in chunks of 64 (four K=16 MMAs per
+// chunk) in two buffers so that staging overlaps the MMAs, TMEM accumulator
+// of 256 columns; the epilogue reads
 // TMEM (tcgen05.ld 32x32b) and applies scale, bias, the ReLU-backward mask and
 // ReLU, writing FP32 (pre-activation) and/or BF16 (activation) outputs.
 #include "common.cuh"
@@ -29,9 +32,10 @@ namespace bmm {
 namespace mlp {
 
 constexpr int kBM = 128, kBN = 256, kBK = 64;
-constexpr int kGemmThreads = 128;
+constexpr int kGemmThreads = 256;  // 8 warps stage; in the epilogue warp w reads TMEM lanes
+                                    // 32 (w % 4).., columns 128 (w / 4)..
 constexpr uint32_t kWaitLimit = 1u << 22;
-// 48 KB of operand tiles; asking for more keeps at most two CTAs (2 x 256
+// Two buffers of 48 KB of operand tiles; 100 KB keeps at most two CTAs (2 x 256
 // TMEM columns) resident per SM.
 constexpr size_t kGemmSmem = 100 * 1024;
 
@@ -55,7 +59,16 @@ struct GemmArgs {
     int ksplit;              // K split over gridDim.z: partial z goes to out_f + z * split_stride
     long long split_stride;
     int* err;
+    int a_mode, b_mode;      // staging path per operand (kStage*), chosen on the host
 };
+
+// Staging paths: kStageElem reads element by element with any strides;
+// kStageKVec reads 8 consecutive K elements (K-contiguous rows) as one vector;
+// kStageRVec reads an 8 x 8 block as 8 vectors of 8 consecutive rows
+// (row-contiguous, K-strided sources: the transposed operands of the backward
+// GEMMs) and transposes it in registers.  Vector paths need 16-byte aligned
+// vectors: the base pointer and the strided dimension's stride in bytes.
+constexpr int kStageElem = 0, kStageKVec = 1, kStageRVec = 2;
 
 __device__ __forceinline__ float load_elem(const void* p, int bf16, long long idx) {
     return bf16 ? __bfloat162float(reinterpret_cast<const __nv_bfloat16*>(p)[idx])
@@ -86,11 +99,127 @@ __device__ void stage(unsigned char* dst, int rows, const void* src, int bf16, l
     }
 }
 
+// 8 elements from src[idx ..] (16-byte aligned) as floats.
+__device__ __forceinline__ void load8(const void* p, int bf16, long long idx, float (&v)[8]) {
+    if (bf16) {
+        const uint4 u = *reinterpret_cast<const uint4*>(
+            reinterpret_cast<const __nv_bfloat16*>(p) + idx);
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&u);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float2 f = __bfloat1622float2(h[i]);
+            v[2 * i] = f.x;
+            v[2 * i + 1] = f.y;
+        }
+    } else {
+        const float4 a = *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(p) + idx);
+        const float4 b =
+            *reinterpret_cast<const float4*>(reinterpret_cast<const float*>(p) + idx + 4);
+        v[0] = a.x, v[1] = a.y, v[2] = a.z, v[3] = a.w;
+        v[4] = b.x, v[5] = b.y, v[6] = b.z, v[7] = b.w;
+    }
+}
+
+// Eight values rounded to BF16 (nearest even), packed as one 16-byte chunk.
+__device__ __forceinline__ uint4 pack8(const float (&v)[8]) {
+    uint4 u;
+    __nv_bfloat16* h = reinterpret_cast<__nv_bfloat16*>(&u);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        h[i] = __float2bfloat16_rn(v[i]);
+    return u;
+}
+
+// Vector staging of a rows x kBK tile (see kStageKVec / kStageRVec); partial
+// chunks at the matrix edges go element by element with zero fill.
+__device__ void stage_vec(unsigned char* dst, int rows, int mode, const void* src, int bf16,
+                          long long ld_r, long long ld_k, int row0, int nrows, int k0, int K) {
+    constexpr int KG = kBK / 8;  // 8-element groups along K
+    if (mode == kStageKVec) {
+        // four chunks per thread in flight: all loads first, then convert and store
+        constexpr int B = 4;
+        for (int c0 = threadIdx.x; c0 < rows * KG; c0 += blockDim.x * B) {
+            float v[B][8];
+            uint4 raw[B];
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                const int c = c0 + j * blockDim.x;
+                const int r = c / KG, kg = c % KG;
+                const int gr = row0 + r, gk = k0 + kg * 8;
+                if (c < rows * KG && gr < nrows && gk + 7 < K) {
+                    if (bf16)
+                        raw[j] = *reinterpret_cast<const uint4*>(
+                            reinterpret_cast<const __nv_bfloat16*>(src) + (long long)gr * ld_r + gk);
+                    else
+                        load8(src, 0, (long long)gr * ld_r + gk, v[j]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        v[j][i] = (c < rows * KG && gr < nrows && gk + i < K)
+                                      ? load_elem(src, bf16, (long long)gr * ld_r + gk + i)
+                                      : 0.f;
+                    if (bf16)
+                        raw[j] = pack8(v[j]);
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < B; ++j) {
+                const int c = c0 + j * blockDim.x;
+                if (c >= rows * KG)
+                    break;
+                const int r = c / KG, kg = c % KG;
+                *reinterpret_cast<uint4*>(dst + umma::kmajor_offset(r, kg * 8, kBK)) =
+                    bf16 ? raw[j] : pack8(v[j]);
+            }
+        }
+    } else {
+        const int RG = rows / 8;
+        for (int c = threadIdx.x; c < RG * KG; c += blockDim.x) {
+            const int rg = c % RG, kg = c / RG;  // neighbouring threads: neighbouring rows
+            const int gr = row0 + rg * 8, gk = k0 + kg * 8;
+            float v[8][8];  // v[k][r]
+            if (gr + 7 < nrows && gk + 7 < K) {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk)
+                    load8(src, bf16, gr + (long long)(gk + kk) * ld_k, v[kk]);
+            } else {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk)
+#pragma unroll
+                    for (int rr = 0; rr < 8; ++rr)
+                        v[kk][rr] = (gr + rr < nrows && gk + kk < K)
+                                        ? load_elem(src, bf16, gr + rr + (long long)(gk + kk) * ld_k)
+                                        : 0.f;
+            }
+#pragma unroll
+            for (int rr = 0; rr < 8; ++rr) {
+                float row[8];
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk)
+                    row[kk] = v[kk][rr];
+                *reinterpret_cast<uint4*>(dst + umma::kmajor_offset(rg * 8 + rr, kg * 8, kBK)) =
+                    pack8(row);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ void stage_any(unsigned char* dst, int rows, int mode, const void* src,
+                                          int bf16, long long ld_r, long long ld_k, int row0,
+                                          int nrows, int k0, int K) {
+    if (mode == kStageElem)
+        stage(dst, rows, src, bf16, ld_r, ld_k, row0, nrows, k0, K);
+    else
+        stage_vec(dst, rows, mode, src, bf16, ld_r, ld_k, row0, nrows, k0, K);
+}
+
+// Two operand buffers: the K chunk after the current one is staged while
+// the tensor cores work on the current one; buffer b is refilled only after
+// the MMAs that read it have signalled its mbarrier.
 __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char* sA = smem;
-    unsigned char* sB = smem + kBM * kBK * 2;
-    __shared__ __align__(8) uint64_t mbar;
+    constexpr int kTileA = kBM * kBK * 2, kTileB = kBN * kBK * 2;
+    __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -98,7 +227,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     if (warp == 0)
         umma::tmem_alloc(&tmem_slot, 256);
     if (tid == 0) {
-        umma::mbar_init(umma::smem_u32(&mbar), 1);
+        umma::mbar_init(umma::smem_u32(&mbar[0]), 1);
+        umma::mbar_init(umma::smem_u32(&mbar[1]), 1);
         s_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -112,36 +242,58 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     const int kbeg = blockIdx.z * per;
     const int nk = min(nk_all, kbeg + per);
     float* out_f = g.out_f ? g.out_f + (long long)blockIdx.z * g.split_stride : nullptr;
-    int kc = kbeg;
-    for (; kc < nk; ++kc) {
-        stage(sA, kBM, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M, kc * kBK, g.K);
-        stage(sB, kBN, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N, kc * kBK, g.K);
-        umma::fence_async_smem();
-        __syncthreads();
+    auto sA = [&](int b) { return smem + b * (kTileA + kTileB); };
+    auto sB = [&](int b) { return smem + b * (kTileA + kTileB) + kTileA; };
+    // the k-th commit on a barrier completes its phase k: parity k & 1
+    auto parity_of = [](int i) { return (uint32_t)((i >> 1) & 1); };
+    int last = -1;  // index of the last chunk whose MMAs were committed
+    if (kbeg < nk) {
+        stage_any(sA(0), kBM, g.a_mode, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M, kbeg * kBK, g.K);
+        stage_any(sB(0), kBN, g.b_mode, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N, kbeg * kBK, g.K);
+    }
+    umma::fence_async_smem();
+    __syncthreads();
+    for (int i = 0; kbeg + i < nk; ++i) {
+        const int b = i & 1, kc = kbeg + i;
         if (tid == 0) {
             umma::fence_after_sync();
-            const uint32_t a0 = umma::smem_u32(sA), b0 = umma::smem_u32(sB);
+            const uint32_t a0 = umma::smem_u32(sA(b)), b0 = umma::smem_u32(sB(b));
 #pragma unroll
             for (int s = 0; s < kBK / 16; ++s) {
                 const uint64_t da = umma::smem_desc(a0 + s * 256, 128, (kBK / 8) * 128);
                 const uint64_t db = umma::smem_desc(b0 + s * 256, 128, (kBK / 8) * 128);
-                umma::mma_bf16(tmem, da, db, idesc, (kc > kbeg || s > 0) ? 1u : 0u);
+                umma::mma_bf16(tmem, da, db, idesc, (i > 0 || s > 0) ? 1u : 0u);
             }
-            umma::commit(umma::smem_u32(&mbar));
+            umma::commit(umma::smem_u32(&mbar[b]));
         }
-        if (!umma::mbar_wait(umma::smem_u32(&mbar), (kc - kbeg) & 1, kWaitLimit))
-            s_fail = 1;
+        last = i;
+        if (kc + 1 < nk) {
+            if (i >= 1 && !umma::mbar_wait(umma::smem_u32(&mbar[b ^ 1]), parity_of(i - 1),
+                                           kWaitLimit))
+                s_fail = 1;
+            stage_any(sA(b ^ 1), kBM, g.a_mode, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M,
+                      (kc + 1) * kBK, g.K);
+            stage_any(sB(b ^ 1), kBN, g.b_mode, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N,
+                      (kc + 1) * kBK, g.K);
+        }
+        umma::fence_async_smem();
         __syncthreads();
         if (s_fail)
             break;
     }
+    // all MMAs done: the last commit arrives after every earlier tcgen05 op
+    if (last >= 0 && !s_fail &&
+        !umma::mbar_wait(umma::smem_u32(&mbar[last & 1]), parity_of(last), kWaitLimit))
+        s_fail = 1;
+    __syncthreads();
     umma::fence_after_sync();
     const bool empty = kbeg >= nk;  // this split has no K chunk: its partial is zero
     if (!s_fail) {
-        const int m = m0 + warp * 32 + lane;
-        for (int c = 0; c < kBN / 32; ++c) {
+        const int quarter = warp & 3, half = warp >> 2;
+        const int m = m0 + quarter * 32 + lane;
+        for (int c = half * (kBN / 64); c < (half + 1) * (kBN / 64); ++c) {
             float v[32];
-            umma::tmem_ld32(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c * 32), v);
+            umma::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(c * 32), v);
             if (m >= g.M)
                 continue;
             if (empty)
@@ -169,7 +321,8 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
         if (tid == 0)
             atomicExch(g.err, 1);
         // let the MMAs in flight finish (bounded) before the TMEM is released
-        umma::mbar_wait(umma::smem_u32(&mbar), (kc - kbeg) & 1, kWaitLimit);
+        if (last >= 0)
+            umma::mbar_wait(umma::smem_u32(&mbar[last & 1]), parity_of(last), kWaitLimit);
     }
     umma::fence_before_sync();
     __syncthreads();
@@ -242,15 +395,16 @@ __global__ void loss_sum_kernel(const float* __restrict__ row_loss, int rows, fl
         *loss = part[0];
 }
 
-// Column sums of a [rows][256] matrix (bias gradients).
-__global__ void colsum_kernel(const float* __restrict__ d, int rows, float* __restrict__ out) {
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= kOut)
-        return;
+// Column sums of a [rows][256] matrix (bias gradients), in two fixed-order
+// steps: CTA b sums rows [b * chunk, (b + 1) * chunk) of every column into
+// part[b], then split_reduce_kernel adds the parts in b order.
+__global__ void colsum_part_kernel(const float* __restrict__ d, int rows, int chunk,
+                                   float* __restrict__ part) {
+    const int r0 = blockIdx.x * chunk, r1 = min(rows, r0 + chunk);
     float s = 0.f;
-    for (int r = 0; r < rows; ++r)
-        s += d[(size_t)r * kOut + n];
-    out[n] = s;
+    for (int r = r0; r < r1; ++r)
+        s += d[(size_t)r * kOut + threadIdx.x];
+    part[(size_t)blockIdx.x * kOut + threadIdx.x] = s;
 }
 
 // out[i] = sum over z < splits of part[z * n + i], in z order (deterministic).
@@ -263,6 +417,15 @@ __global__ void split_reduce_kernel(const float* __restrict__ part, int splits, 
     for (int z = 0; z < splits; ++z)
         s += part[(size_t)z * n + i];
     out[i] = s;
+}
+
+// Bias gradient: column sums of d[rows][256] into out[256] (part: scratch of
+// at most 8192 x 256 floats).
+void colsum(const float* d, int rows, float* part, float* out, cudaStream_t s) {
+    const int chunk = std::max(128, (rows + 8191) / 8192);
+    const int parts = std::max(1, (rows + chunk - 1) / chunk);
+    colsum_part_kernel<<<parts, kOut, 0, s>>>(d, rows, chunk, part);
+    split_reduce_kernel<<<1, kOut, 0, s>>>(part, parts, kOut, out);
 }
 
 // Adam (Kingma & Ba) with bias correction on the FP32 master parameters.
@@ -288,6 +451,19 @@ using namespace bmm::mlp;
 
 namespace {
 
+// The vector paths need 16-byte aligned 8-element vectors: a 16-byte aligned
+// base and a stride of the other dimension that keeps every vector aligned.
+int stage_mode(const void* p, int bf16, long long ld_r, long long ld_k) {
+    const long long vec = bf16 ? 8 : 4;  // elements per 16 bytes
+    if ((reinterpret_cast<uintptr_t>(p) & 15) != 0)
+        return kStageElem;
+    if (ld_k == 1 && ld_r % vec == 0)
+        return kStageKVec;
+    if (ld_r == 1 && ld_k % vec == 0)
+        return kStageRVec;
+    return kStageElem;
+}
+
 int gemm_launch(const GemmArgs& a, cudaStream_t s) {
     static thread_local int attr_dev = -1;
     int dev = -1;
@@ -297,8 +473,11 @@ int gemm_launch(const GemmArgs& a, cudaStream_t s) {
                                           (int)kGemmSmem));
         attr_dev = dev;
     }
+    GemmArgs g = a;
+    g.a_mode = stage_mode(a.A, a.a_bf16, a.lda_m, a.lda_k);
+    g.b_mode = stage_mode(a.B, a.b_bf16, a.ldb_n, a.ldb_k);
     dim3 grid((a.M + kBM - 1) / kBM, (a.N + kBN - 1) / kBN, a.ksplit > 1 ? a.ksplit : 1);
-    gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(a);
+    gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(g);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return fail(BMM_ECUDA, "mlp: gemm launch failed: %s", cudaGetErrorString(e));
@@ -425,7 +604,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     // dW3 = dZ3^T H2, db3
     GemmArgs a = gemm_args(h->dz3, 0, 1, kOut, h->h2, 1, 1, kHid, kOut, kHid, rows, h->err);
     BMM_TRY(gemm_wgrad(a, h->g + kW3, h->part, s));
-    colsum_kernel<<<1, 256, 0, s>>>(h->dz3, rows, h->g + kB3);
+    colsum(h->dz3, rows, h->part, h->g + kB3, s);
     // dZ2 = (dZ3 W3) * (Z2 > 0)
     a = gemm_args(h->dz3, 0, kOut, 1, h->w + kW3, 0, 1, kHid, rows, kHid, kOut, h->err);
     a.relu_mask = h->z2;
@@ -436,7 +615,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     // dW2 = dZ2^T H1, db2
     a = gemm_args(h->dz2, 0, 1, kHid, h->h1, 1, 1, kHid, kHid, kHid, rows, h->err);
     BMM_TRY(gemm_wgrad(a, h->g + kW2, h->part, s));
-    colsum_kernel<<<1, 256, 0, s>>>(h->dz2, rows, h->g + kB2);
+    colsum(h->dz2, rows, h->part, h->g + kB2, s);
     // dZ1 = (dZ2 W2) * (Z1 > 0)
     a = gemm_args(h->dz2, 0, kHid, 1, h->w + kW2, 0, 1, kHid, rows, kHid, kHid, h->err);
     a.relu_mask = h->z1;
@@ -447,7 +626,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     // dW1 = dZ1^T X (N = 512: two column tiles), db1
     a = gemm_args(h->dz1, 0, 1, kHid, X, x_bf16, 1, kIn, kHid, kIn, rows, h->err);
     BMM_TRY(gemm_wgrad(a, h->g + kW1, h->part, s));
-    colsum_kernel<<<1, 256, 0, s>>>(h->dz1, rows, h->g + kB1);
+    colsum(h->dz1, rows, h->part, h->g + kB1, s);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return fail(BMM_ECUDA, "mlp: backward launch failed: %s", cudaGetErrorString(e));
