@@ -39,6 +39,9 @@ the planted 512 x 65536 matrix: ``value`` from the device synergy table,
 payload parsed on the device, BitMatrix.from_text and a binary file loaded
 into device memory end to end.
 
+``--workload mlp`` (1 GPU) measures the proposal network's tcgen05 GEMMs
+(forward and training step on 16384 resident rows).
+
 ``--workload ga`` (1 GPU) measures the island-model GA instead: the planted
 256 x 8192 matrix (density 0.01, 5000 scrambles, seed 7), 64 islands x 256,
 ring migration every 20 generations, stop at the planted weight or the
@@ -821,6 +824,73 @@ def run_io(args):
     return 0
 
 
+def run_mlp(args):
+    """The proposal network's tcgen05 GEMMs: forward passes and training steps
+    (forward, backward, Adam) on 16384 resident query rows, CUDA-event timed
+    on the network's stream; TFLOP/s of the GEMM work (forward 2 x rows x
+    262144 flops, a training step 3x that)."""
+    import ctypes
+
+    import torch
+
+    from bmmpy_b200 import _native as N
+
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "the proposal network has no counterpart in the "
+                                         "reference (its GA mutates uniformly)"}))
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    rows = 16384
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.rand((rows, 512), generator=g, device=dev)
+    t = torch.rand((rows, 256), generator=g, device=dev)
+    t /= t.sum(1, keepdim=True)
+    logits = torch.empty((rows, 256), device=dev)
+    torch.cuda.synchronize()
+    L = N.lib()
+    h = ctypes.c_void_p()
+    N.check(L.bmm_mlp_create_on_stream(1, 1e-3, stream.cuda_stream, ctypes.byref(h)))
+    flops_fwd = 2.0 * rows * (512 * 256 + 256 * 256 + 256 * 256)
+    out = {}
+    for name, fn, flops in (
+            ("forward", lambda: L.bmm_mlp_forward_dev(h, x.data_ptr(), rows, logits.data_ptr()),
+             flops_fwd),
+            ("train_step", lambda: L.bmm_mlp_train_dev(h, x.data_ptr(), t.data_ptr(), rows, 1),
+             3 * flops_fwd)):
+        for _ in range(args.warmup):
+            N.check(fn())
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.steps):
+            N.check(fn())
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = a.elapsed_time(b) / args.steps
+        out[name] = {"ms": ms, "tflops": flops / (ms / 1e3) / 1e12}
+    N.check(L.bmm_mlp_destroy(h))
+    peak = 1590.0
+    line = {"metric": "proposal-network GEMM TFLOP/s (BF16 operands, FP32 accumulate, tcgen05)",
+            "value": out["train_step"]["tflops"], "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["train_step"]["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16",
+            "data": "synthetic features and targets (torch.rand, seed 0)",
+            "config": {"workload": "512-256-256-256 MLP, 16384 query rows resident on the "
+                                   "device: training step (forward, backward, Adam) and forward"},
+            "forward": out["forward"], "train_step": out["train_step"],
+            "roofline": {"bound": "tensor", "achieved": out["train_step"]["tflops"],
+                         "peak": peak, "unit": "TFLOP/s",
+                         "frac": out["train_step"]["tflops"] / peak,
+                         "peak_source": "fallback 1.59 PFLOP/s dense BF16 (no measured peaks "
+                                        "file)", "traffic": None}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 def main():
     ap = argparse.ArgumentParser()
@@ -829,7 +899,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa", "io"])
+    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa", "io", "mlp"])
     ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
     ap.add_argument("--seeds", type=int, default=2, help="GA: seeds per variant")
     ap.add_argument("--islands", type=int, default=64)
@@ -846,6 +916,8 @@ def main():
         return run_sa(args)
     if args.workload == "io":
         return run_io(args)
+    if args.workload == "mlp":
+        return run_mlp(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -192,6 +192,9 @@ SIGNATURES = {
     "bmm_mlp_grads": [_vp, _f32p, _f32p, _sz, _f32p, _f32p],
     "bmm_mlp_train": [_vp, _f32p, _f32p, _sz, C.c_int, _f32p],
     "bmm_mlp_gemm": [_f32p, _f32p, C.c_int, C.c_int, C.c_int, _f32p],
+    "bmm_mlp_create_on_stream": [C.c_uint64, C.c_float, _vp, C.POINTER(_vp)],
+    "bmm_mlp_forward_dev": [_vp, _vp, _sz, _vp],
+    "bmm_mlp_train_dev": [_vp, _vp, _vp, _sz, C.c_int],
     "bmm_exact_basis": [_u64p, _sz, _sz, _u32p, _sz, C.POINTER(ExactBasisConfig_t),
                         C.POINTER(ExactBasisResult_t), _u32p, _u32p],
     "bmm_basis_weight_counts": [_u64p, _sz, _sz, _u32p, _sz, _u64p],

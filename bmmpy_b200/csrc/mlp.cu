@@ -804,6 +804,50 @@ BMM_API int bmm_mlp_set_params(bmm_mlp* h, const float* params) {
     return BMM_OK;
 }
 
+BMM_API int bmm_mlp_create_on_stream(uint64_t seed, float learning_rate, void* stream,
+                                     bmm_mlp** out) {
+    clear_error();
+    if (!out || !stream)
+        return fail(BMM_EINVAL, "mlp: null output, or the null stream (pass a created stream)");
+    *out = nullptr;
+    if (!(learning_rate > 0.f))
+        return fail(BMM_EINVAL, "mlp: learning rate must be positive");
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    return bmm::mlp::create(seed, learning_rate, (cudaStream_t)stream, out);
+}
+
+// Device-pointer forms: enqueued on the handle's stream, no synchronisation.
+BMM_API int bmm_mlp_forward_dev(bmm_mlp* h, const float* x, size_t rows, float* logits) {
+    clear_error();
+    if (!h || (rows && (!x || !logits)))
+        return fail(BMM_EINVAL, "mlp: null argument");
+    if (rows == 0)
+        return BMM_OK;
+    if (rows > (1u << 24))
+        return fail(BMM_EINVAL, "mlp: too many rows");
+    BMM_TRY(ensure_cap(h, rows));
+    BMM_TRY(forward_dev(h, x, 0, (int)rows, nullptr));
+    BMM_CUDA_TRY(cudaMemcpyAsync(logits, h->z3, rows * kOut * 4, cudaMemcpyDeviceToDevice,
+                                 h->stream));
+    return BMM_OK;
+}
+
+BMM_API int bmm_mlp_train_dev(bmm_mlp* h, const float* x, const float* target, size_t rows,
+                              int steps) {
+    clear_error();
+    if (!h || !x || !target || rows == 0 || steps < 1)
+        return fail(BMM_EINVAL, "mlp: null argument, no rows or no steps");
+    if (rows > (1u << 24))
+        return fail(BMM_EINVAL, "mlp: too many rows");
+    BMM_TRY(ensure_cap(h, rows));
+    for (int s = 0; s < steps; ++s)
+        BMM_TRY(train_step_dev(h, x, 0, target, (int)rows));
+    return BMM_OK;
+}
+
 BMM_API int bmm_mlp_forward(bmm_mlp* h, const float* x, size_t rows, float* logits) {
     clear_error();
     if (!h || (rows && (!x || !logits)))

@@ -380,6 +380,16 @@ BMM_API int bmm_mlp_train(bmm_mlp* h, const float* x, const float* target, size_
                           int steps, float* loss);
 /* C[M][N] = bf16(A[M][K]) . bf16(B[N][K])^T in FP32 on the tensor cores */
 BMM_API int bmm_mlp_gemm(const float* A, const float* B, int M, int N, int K, float* C);
+/* A network whose work runs on the caller's (created, non-null) stream; the
+ * stream is not destroyed with the network. */
+BMM_API int bmm_mlp_create_on_stream(uint64_t seed, float learning_rate, void* stream,
+                                     bmm_mlp** out);
+/* Device-pointer forms of forward / train: x [rows][512], target and logits
+ * [rows][256] in device memory; enqueued on the network's stream without
+ * synchronisation (errors of the kernels surface at the next host call). */
+BMM_API int bmm_mlp_forward_dev(bmm_mlp* h, const float* x, size_t rows, float* logits);
+BMM_API int bmm_mlp_train_dev(bmm_mlp* h, const float* x, const float* target, size_t rows,
+                              int steps);
 
 /* ---- exact minimum-weight basis of a window ------------------------------
  * ExactBasisSolverConfig / ExactBasisResult of
