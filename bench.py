@@ -390,7 +390,8 @@ def run_mitm(args):
     start = m.weight()
     searcher = bmm.MitmFwhtSearch(max_candidates=64)
     applier = bmm.GreedyApplier(1)
-    nwin = C3["rows"] // C3["window"]
+    window = args.window or C3["window"]
+    nwin = C3["rows"] // window
     sweeps = []
     rng = np.random.default_rng(C3["seed"])
     dev = bmm.DeviceMatrix(m)  # the matrix stays on the device for the whole run
@@ -401,7 +402,7 @@ def run_mitm(args):
     weight = start
     while time.perf_counter() - t0 < args.cap and idle < 4:
         perm = rng.permutation(C3["rows"])
-        wins = [sorted(int(r) for r in perm[C3["window"] * j: C3["window"] * (j + 1)])
+        wins = [sorted(int(r) for r in perm[window * j: window * (j + 1)])
                 for j in range(nwin)]
         res = dev.search_apply(wins, searcher=searcher, applier=applier)
         windows += nwin
@@ -420,11 +421,12 @@ def run_mitm(args):
         "dtype": "int32 spectra", "data": "synthetic planted matrix (xorshift64 seed 2)",
         "vs_baseline": None,
         "config": {"workload": "planted 512x65536 matrix (density 0.02, 2000 scrambles, seed 2), "
-                               "sweeps of 16 random 32-row windows, MitmFwhtSearch(k=64) + "
-                               "GreedyApplier(1) as one device-resident sweep per call",
-                   "cap_s": args.cap},
+                               f"sweeps of {nwin} random {window}-row windows, "
+                               "MitmFwhtSearch(k=64) + GreedyApplier(1) as one device-resident "
+                               "sweep per call",
+                   "cap_s": args.cap, "window": window},
         "planted_weight": planted, "start_weight": start,
-        "combos_per_s": windows * float(1 << C3["window"]) / search_s,
+        "combos_per_s": windows * float(1 << window) / search_s,
         "seconds_per_window": search_s / windows,
         "sweeps": sweeps,
     }
@@ -901,6 +903,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa", "io", "mlp"])
     ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
+    ap.add_argument("--window", type=int, default=0,
+                    help="mitm: window rows (default 32; one sweep = rows / window windows)")
     ap.add_argument("--seeds", type=int, default=2, help="GA: seeds per variant")
     ap.add_argument("--islands", type=int, default=64)
     ap.add_argument("--population", type=int, default=256)
