@@ -111,3 +111,37 @@ def test_adam_training_follows_oracle_and_learns(net):
     # and it learns: 200 more steps cut the loss well below the start
     N.check(N.lib().bmm_mlp_train(net, N.f32p(X), N.f32p(T), 512, 200, C.byref(got_loss)))
     assert got_loss.value < 0.8 * losses[0]
+
+
+def test_device_entry_points_match_host_ones():
+    # bmm_mlp_create_on_stream + bmm_mlp_forward_dev / bmm_mlp_train_dev run the
+    # same kernels as the host-pointer entry points, on the caller's stream:
+    # same logits and, after the same training steps, the same parameters
+    import torch
+
+    X, T = _inputs(700, 9)
+    stream = torch.cuda.Stream()
+    L = N.lib()
+    a, b = C.c_void_p(), C.c_void_p()
+    N.check(L.bmm_mlp_create(5, 1e-3, C.byref(a)))
+    N.check(L.bmm_mlp_create_on_stream(5, 1e-3, stream.cuda_stream, C.byref(b)))
+    try:
+        dx, dt = torch.from_numpy(X).cuda(), torch.from_numpy(T).cuda()
+        dl = torch.empty((700, 256), device="cuda")
+        torch.cuda.synchronize()
+        want = np.zeros((700, 256), np.float32)
+        N.check(L.bmm_mlp_forward(a, N.f32p(X), 700, N.f32p(want)))
+        N.check(L.bmm_mlp_forward_dev(b, dx.data_ptr(), 700, dl.data_ptr()))
+        stream.synchronize()
+        assert np.array_equal(dl.cpu().numpy(), want)
+        loss = np.zeros(1, np.float32)
+        N.check(L.bmm_mlp_train(a, N.f32p(X), N.f32p(T), 700, 3, N.f32p(loss)))
+        N.check(L.bmm_mlp_train_dev(b, dx.data_ptr(), dt.data_ptr(), 700, 3))
+        stream.synchronize()
+        assert np.array_equal(_params(a), _params(b))
+        with pytest.raises(ValueError, match="null stream"):
+            h = C.c_void_p()
+            N.check(L.bmm_mlp_create_on_stream(5, 1e-3, None, C.byref(h)))
+    finally:
+        L.bmm_mlp_destroy(a)
+        L.bmm_mlp_destroy(b)
