@@ -17,7 +17,8 @@
 //  4. the improving examples, compacted in query order, train the network
 //     with `train_steps` Adam steps.
 // The share of learned windows adapts to the measured success rates of
-// learned and uniform windows (the uniform draw stays as fallback and judge).
+// learned and uniform windows (the uniform draw stays as the fallback and the
+// yardstick the learned windows are compared with).
 // All random draws are counter-based hashes of (seed, generation, query), so
 // a run is deterministic for a seed.
 #include "common.cuh"
@@ -448,7 +449,7 @@ int propose_generation(bmm_ga* g) {
             if (err)
                 return fail(BMM_ETIMEOUT, "ga: a tensor-core wait timed out in the proposal network");
         }
-        // fallback and judge: decayed success counts of both window sources;
+        // learned share: decayed success counts of both window sources;
         // the learned share moves towards the better one
         const unsigned long long* k = g->h_counters;
         for (int src = 0; src < 2; ++src) {
