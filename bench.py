@@ -90,6 +90,25 @@ def workload_config(n):
 
 
 # ---------------------------------------------------------------------------
+def max_over_ranks(value, dist=None, device="cpu"):
+    """The largest per-rank value over all ranks (a job's time is its slowest
+    rank's); with no process group, the value itself."""
+    if not dist:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_throughput(world, units_per_rank, seconds):
+    """Whole-job rate of a weak-scaling run: every rank processed the same
+    number of units (its own instance) within the slowest rank's time."""
+    return world * units_per_rank / seconds
+
+
+# ---------------------------------------------------------------------------
 def clock_sampler(uuid):
     """Sample SM clocks and throttle reasons while the timed region runs."""
     fields = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -990,12 +1009,9 @@ def main():
         dist.barrier()
     clocks = clock_summary(sampler)
     total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_ms = float(t.item())
+    max_ms = max_over_ranks(total_ms, dist, dev)
     combos_step = ROWS * COMBOS_PER_TARGET
-    value = world * combos_step * args.steps / (max_ms / 1e3)
+    value = weak_throughput(world, combos_step * args.steps, max_ms / 1e3)
 
     # correctness of what was timed: rank 0 instance == the golden answer
     got_w = d_w.cpu().numpy().view(np.uint32)
@@ -1021,10 +1037,7 @@ def main():
     for _ in range(e_steps):
         em, ew = T.gray_targets(hm, pt, po)
     e_dt = time.perf_counter() - t0
-    e = torch.tensor([e_dt], dtype=torch.float64, device=dev)
-    if dist:
-        dist.all_reduce(e, op=dist.ReduceOp.MAX)
-    e2e_value = world * combos_step * e_steps / float(e.item())
+    e2e_value = weak_throughput(world, combos_step * e_steps, max_over_ranks(e_dt, dist, dev))
     assert np.array_equal(ew, got_w), "e2e and resident results differ"
 
     # roofline: XOR+POPC word rate of the targets kernel vs the measured probe
