@@ -60,10 +60,13 @@ struct GemmArgs {
     long long split_stride;
     int* err;
     int a_mode, b_mode;      // staging path per operand (kStage*), chosen on the host
+    int vec_f, vec_b, vec_mask;  // epilogue rows 16-byte aligned: vector stores / loads
 };
 
 // Staging paths: kStageElem reads element by element with any strides;
-// kStageKVec reads 8 consecutive K elements (K-contiguous rows) as one vector;
+// kStageKVec reads 8 consecutive K elements (K-contiguous rows) as one vector
+// (BF16 sources by a 16-byte cp.async straight into place, FP32 ones through
+// registers, rounded);
 // kStageRVec reads an 8 x 8 block as 8 vectors of 8 consecutive rows
 // (row-contiguous, K-strided sources: the transposed operands of the backward
 // GEMMs) and transposes it in registers.  Vector paths need 16-byte aligned
@@ -147,11 +150,18 @@ __device__ void stage_vec(unsigned char* dst, int rows, int mode, const void* sr
                 const int r = c / KG, kg = c % KG;
                 const int gr = row0 + r, gk = k0 + kg * 8;
                 if (c < rows * KG && gr < nrows && gk + 7 < K) {
-                    if (bf16)
-                        raw[j] = *reinterpret_cast<const uint4*>(
-                            reinterpret_cast<const __nv_bfloat16*>(src) + (long long)gr * ld_r + gk);
-                    else
+                    if (bf16) {
+                        // BF16 source: copied asynchronously straight into place
+                        const int r = c / KG, kg = c % KG;
+                        const uint32_t sa = (uint32_t)__cvta_generic_to_shared(
+                            dst + umma::kmajor_offset(r, kg * 8, kBK));
+                        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa),
+                                     "l"(reinterpret_cast<const __nv_bfloat16*>(src) +
+                                         (long long)gr * ld_r + gk)
+                                     : "memory");
+                    } else {
                         load8(src, 0, (long long)gr * ld_r + gk, v[j]);
+                    }
                 } else {
 #pragma unroll
                     for (int i = 0; i < 8; ++i)
@@ -168,6 +178,9 @@ __device__ void stage_vec(unsigned char* dst, int rows, int mode, const void* sr
                 if (c >= rows * KG)
                     break;
                 const int r = c / KG, kg = c % KG;
+                const int gr = row0 + r, gk = k0 + kg * 8;
+                if (bf16 && gr < nrows && gk + 7 < K)
+                    continue;  // written by its cp.async
                 *reinterpret_cast<uint4*>(dst + umma::kmajor_offset(r, kg * 8, kBK)) =
                     bf16 ? raw[j] : pack8(v[j]);
             }
@@ -248,9 +261,10 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     auto parity_of = [](int i) { return (uint32_t)((i >> 1) & 1); };
     int last = -1;  // index of the last chunk whose MMAs were committed
     if (kbeg < nk) {
-        stage_any(sA(0), kBM, g.a_mode, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M, kbeg * kBK, g.K);
         stage_any(sB(0), kBN, g.b_mode, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N, kbeg * kBK, g.K);
+        stage_any(sA(0), kBM, g.a_mode, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M, kbeg * kBK, g.K);
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     umma::fence_async_smem();
     __syncthreads();
     for (int i = 0; kbeg + i < nk; ++i) {
@@ -271,11 +285,12 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
             if (i >= 1 && !umma::mbar_wait(umma::smem_u32(&mbar[b ^ 1]), parity_of(i - 1),
                                            kWaitLimit))
                 s_fail = 1;
-            stage_any(sA(b ^ 1), kBM, g.a_mode, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M,
-                      (kc + 1) * kBK, g.K);
             stage_any(sB(b ^ 1), kBN, g.b_mode, g.B, g.b_bf16, g.ldb_n, g.ldb_k, n0, g.N,
                       (kc + 1) * kBK, g.K);
+            stage_any(sA(b ^ 1), kBM, g.a_mode, g.A, g.a_bf16, g.lda_m, g.lda_k, m0, g.M,
+                      (kc + 1) * kBK, g.K);
         }
+        asm volatile("cp.async.wait_all;" ::: "memory");
         umma::fence_async_smem();
         __syncthreads();
         if (s_fail)
@@ -300,21 +315,66 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
 #pragma unroll
                 for (int i = 0; i < 32; ++i)
                     v[i] = 0.f;
+            // 32 consecutive outputs of row m: 16-byte vector loads and stores
+            // where the host found the rows aligned, element by element else
+            const int nb = n0 + c * 32;
+            const bool full = nb + 31 < g.N;
 #pragma unroll
             for (int i = 0; i < 32; ++i) {
-                const int n = n0 + c * 32 + i;
-                if (n >= g.N)
-                    continue;
                 float val = v[i] * g.scale;
-                if (g.bias)
-                    val += g.bias[n];
-                if (g.relu_mask && !(g.relu_mask[(long long)m * g.ldm + n] > 0.f))
-                    val = 0.f;
-                if (out_f)
-                    out_f[(long long)m * g.ldo_f + n] = val;
-                if (g.out_b)
-                    g.out_b[(long long)m * g.ldo_b + n] =
-                        __float2bfloat16_rn(g.relu ? fmaxf(val, 0.f) : val);
+                if (g.bias && nb + i < g.N)
+                    val += g.bias[nb + i];
+                v[i] = val;
+            }
+            if (g.relu_mask) {
+                const float* mrow = g.relu_mask + (long long)m * g.ldm + nb;
+                if (full && g.vec_mask) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const float4 mk = reinterpret_cast<const float4*>(mrow)[q];
+                        if (!(mk.x > 0.f)) v[4 * q] = 0.f;
+                        if (!(mk.y > 0.f)) v[4 * q + 1] = 0.f;
+                        if (!(mk.z > 0.f)) v[4 * q + 2] = 0.f;
+                        if (!(mk.w > 0.f)) v[4 * q + 3] = 0.f;
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (nb + i < g.N && !(mrow[i] > 0.f))
+                            v[i] = 0.f;
+                }
+            }
+            if (out_f) {
+                float* orow = out_f + (long long)m * g.ldo_f + nb;
+                if (full && g.vec_f) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        reinterpret_cast<float4*>(orow)[q] =
+                            make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (nb + i < g.N)
+                            orow[i] = v[i];
+                }
+            }
+            if (g.out_b) {
+                __nv_bfloat16* brow = g.out_b + (long long)m * g.ldo_b + nb;
+                if (full && g.vec_b) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        float b8[8];
+#pragma unroll
+                        for (int i = 0; i < 8; ++i)
+                            b8[i] = g.relu ? fmaxf(v[8 * q + i], 0.f) : v[8 * q + i];
+                        reinterpret_cast<uint4*>(brow)[q] = pack8(b8);
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (nb + i < g.N)
+                            brow[i] = __float2bfloat16_rn(g.relu ? fmaxf(v[i], 0.f) : v[i]);
+                }
             }
         }
     } else {
@@ -429,7 +489,9 @@ void colsum(const float* d, int rows, float* part, float* out, cudaStream_t s) {
 }
 
 // Adam (Kingma & Ba) with bias correction on the FP32 master parameters.
-__global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+// Also rewrites the BF16 copy of the weights that the GEMMs read.
+__global__ void adam_kernel(float* __restrict__ w, __nv_bfloat16* __restrict__ wb,
+                            float* __restrict__ m, float* __restrict__ v,
                             const float* __restrict__ grad, size_t n, float lr, float b1, float b2,
                             float eps, float c1, float c2) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -440,7 +502,18 @@ __global__ void adam_kernel(float* __restrict__ w, float* __restrict__ m, float*
     const float vi = b2 * v[i] + (1.f - b2) * g * g;
     m[i] = mi;
     v[i] = vi;
-    w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    wb[i] = __float2bfloat16_rn(wi);
+}
+
+// The BF16 copy of the weights: the same rounding the GEMM staging applies to
+// FP32 operands, done once per update instead of once per CTA and K chunk.
+__global__ void to_bf16_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ wb,
+                               size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        wb[i] = __float2bfloat16_rn(w[i]);
 }
 
 }  // namespace mlp
@@ -476,6 +549,11 @@ int gemm_launch(const GemmArgs& a, cudaStream_t s) {
     GemmArgs g = a;
     g.a_mode = stage_mode(a.A, a.a_bf16, a.lda_m, a.lda_k);
     g.b_mode = stage_mode(a.B, a.b_bf16, a.ldb_n, a.ldb_k);
+    auto al16 = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; };
+    g.vec_f = a.out_f && al16(a.out_f) && a.ldo_f % 4 == 0 &&
+              (a.ksplit <= 1 || a.split_stride % 4 == 0);
+    g.vec_b = a.out_b && al16(a.out_b) && a.ldo_b % 8 == 0;
+    g.vec_mask = a.relu_mask && al16(a.relu_mask) && a.ldm % 4 == 0;
     dim3 grid((a.M + kBM - 1) / kBM, (a.N + kBN - 1) / kBN, a.ksplit > 1 ? a.ksplit : 1);
     gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(g);
     const cudaError_t e = cudaGetLastError();
@@ -572,7 +650,7 @@ namespace mlp {
 // Forward pass of `rows` inputs X (FP32 or BF16, row stride kIn) into the
 // handle's scratch: z1/h1, z2/h2, logits z3 (or `logits` if given).
 int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) {
-    GemmArgs a = gemm_args(X, x_bf16, kIn, 1, h->w + kW1, 0, kIn, 1, rows, kHid, kIn, h->err);
+    GemmArgs a = gemm_args(X, x_bf16, kIn, 1, h->wb + kW1, 1, kIn, 1, rows, kHid, kIn, h->err);
     a.bias = h->w + kB1;
     a.relu = 1;
     a.out_f = h->z1;
@@ -580,7 +658,7 @@ int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) 
     a.out_b = h->h1;
     a.ldo_b = kHid;
     BMM_TRY(gemm_launch(a, h->stream));
-    a = gemm_args(h->h1, 1, kHid, 1, h->w + kW2, 0, kHid, 1, rows, kHid, kHid, h->err);
+    a = gemm_args(h->h1, 1, kHid, 1, h->wb + kW2, 1, kHid, 1, rows, kHid, kHid, h->err);
     a.bias = h->w + kB2;
     a.relu = 1;
     a.out_f = h->z2;
@@ -588,7 +666,7 @@ int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) 
     a.out_b = h->h2;
     a.ldo_b = kHid;
     BMM_TRY(gemm_launch(a, h->stream));
-    a = gemm_args(h->h2, 1, kHid, 1, h->w + kW3, 0, kHid, 1, rows, kOut, kHid, h->err);
+    a = gemm_args(h->h2, 1, kHid, 1, h->wb + kW3, 1, kHid, 1, rows, kOut, kHid, h->err);
     a.bias = h->w + kB3;
     a.out_f = logits ? logits : h->z3;
     a.ldo_f = kOut;
@@ -606,7 +684,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     BMM_TRY(gemm_wgrad(a, h->g + kW3, h->part, s));
     colsum(h->dz3, rows, h->part, h->g + kB3, s);
     // dZ2 = (dZ3 W3) * (Z2 > 0)
-    a = gemm_args(h->dz3, 0, kOut, 1, h->w + kW3, 0, 1, kHid, rows, kHid, kOut, h->err);
+    a = gemm_args(h->dz3, 0, kOut, 1, h->wb + kW3, 1, 1, kHid, rows, kHid, kOut, h->err);
     a.relu_mask = h->z2;
     a.ldm = kHid;
     a.out_f = h->dz2;
@@ -617,7 +695,7 @@ int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows
     BMM_TRY(gemm_wgrad(a, h->g + kW2, h->part, s));
     colsum(h->dz2, rows, h->part, h->g + kB2, s);
     // dZ1 = (dZ2 W2) * (Z1 > 0)
-    a = gemm_args(h->dz2, 0, kHid, 1, h->w + kW2, 0, 1, kHid, rows, kHid, kHid, h->err);
+    a = gemm_args(h->dz2, 0, kHid, 1, h->wb + kW2, 1, 1, kHid, rows, kHid, kHid, h->err);
     a.relu_mask = h->z1;
     a.ldm = kHid;
     a.out_f = h->dz1;
@@ -638,7 +716,7 @@ int adam_dev(bmm_mlp* h) {
     const float c1 = 1.f - (float)std::pow((double)h->b1, (double)h->step);
     const float c2 = 1.f - (float)std::pow((double)h->b2, (double)h->step);
     adam_kernel<<<(unsigned)((kParams + 255) / 256), 256, 0, h->stream>>>(
-        h->w, h->m, h->v, h->g, kParams, h->lr, h->b1, h->b2, h->eps, c1, c2);
+        h->w, h->wb, h->m, h->v, h->g, kParams, h->lr, h->b1, h->b2, h->eps, c1, c2);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return fail(BMM_ECUDA, "mlp: adam launch failed: %s", cudaGetErrorString(e));
@@ -690,6 +768,7 @@ void mlp_free(bmm_mlp* h) {
         cudaFree(p);
     cudaFree(h->h1);
     cudaFree(h->h2);
+    cudaFree(h->wb);
     cudaFree(h->err);
     if (h->stream && h->owns_stream)
         cudaStreamDestroy(h->stream);
@@ -747,19 +826,31 @@ int create(uint64_t seed, float learning_rate, cudaStream_t stream, bmm_mlp** ou
         if (e == cudaSuccess)
             e = cudaMalloc(q, kParams * 4);
     if (e == cudaSuccess)
+        e = cudaMalloc(&h->wb, kParams * 2);
+    if (e == cudaSuccess)
         e = cudaMalloc(&h->part, (size_t)16 * kHid * kIn * 4);
     if (e == cudaSuccess)
         e = cudaMalloc(&h->loss, 4);
     if (e == cudaSuccess)
         e = cudaMalloc(&h->err, 4);
+    // everything on the network's stream, in order: the BF16 copy is made
+    // from the uploaded weights (a pageable cudaMemcpy may return before its
+    // DMA lands, and the network's stream need not wait for it)
     if (e == cudaSuccess)
-        e = cudaMemcpy(h->w, p.data(), kParams * 4, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(h->w, p.data(), kParams * 4, cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess)
-        e = cudaMemset(h->m, 0, kParams * 4);
+        e = cudaMemsetAsync(h->m, 0, kParams * 4, h->stream);
     if (e == cudaSuccess)
-        e = cudaMemset(h->v, 0, kParams * 4);
+        e = cudaMemsetAsync(h->v, 0, kParams * 4, h->stream);
     if (e == cudaSuccess)
-        e = cudaMemset(h->err, 0, 4);
+        e = cudaMemsetAsync(h->err, 0, 4, h->stream);
+    if (e == cudaSuccess) {
+        to_bf16_kernel<<<(unsigned)((kParams + 255) / 256), 256, 0, h->stream>>>(h->w, h->wb,
+                                                                               kParams);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         mlp_free(h);
@@ -797,6 +888,9 @@ BMM_API int bmm_mlp_set_params(bmm_mlp* h, const float* params) {
     if (!h || !params)
         return fail(BMM_EINVAL, "mlp: null argument");
     BMM_CUDA_TRY(cudaMemcpyAsync(h->w, params, kParams * 4, cudaMemcpyHostToDevice, h->stream));
+    to_bf16_kernel<<<(unsigned)((kParams + 255) / 256), 256, 0, h->stream>>>(h->w, h->wb,
+                                                                           kParams);
+    BMM_CUDA_TRY(cudaGetLastError());
     BMM_CUDA_TRY(cudaMemsetAsync(h->m, 0, kParams * 4, h->stream));
     BMM_CUDA_TRY(cudaMemsetAsync(h->v, 0, kParams * 4, h->stream));
     BMM_CUDA_TRY(cudaStreamSynchronize(h->stream));

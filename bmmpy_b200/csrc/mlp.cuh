@@ -24,6 +24,7 @@ struct bmm_mlp {
     cudaStream_t stream = nullptr;
     bool owns_stream = true;
     float* w = nullptr;  // kParams
+    __nv_bfloat16* wb = nullptr;  // kParams: w rounded to BF16, rewritten whenever w changes
     float* m = nullptr;
     float* v = nullptr;
     float* g = nullptr;
