@@ -438,9 +438,12 @@ __global__ void xent_kernel(const float* __restrict__ logits, const float* __res
         row_loss[r] = l * inv;
 }
 
-// *loss = sum of row_loss in row order (one CTA, fixed reduction tree).
-__global__ void loss_sum_kernel(const float* __restrict__ row_loss, int rows, float* loss) {
-    __shared__ float part[256];
+// *loss = sum of row_loss (one CTA of kLossThreads, fixed strided order and
+// reduction tree: deterministic).
+constexpr int kLossThreads = 1024;
+__global__ void __launch_bounds__(kLossThreads)
+    loss_sum_kernel(const float* __restrict__ row_loss, int rows, float* loss) {
+    __shared__ float part[kLossThreads];
     float s = 0.f;
     for (int r = threadIdx.x; r < rows; r += blockDim.x)
         s += row_loss[r];
@@ -678,7 +681,7 @@ int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) 
 int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows) {
     cudaStream_t s = h->stream;
     xent_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(h->z3, T, h->dz3, h->row_loss, rows);
-    loss_sum_kernel<<<1, 256, 0, s>>>(h->row_loss, rows, h->loss);
+    loss_sum_kernel<<<1, kLossThreads, 0, s>>>(h->row_loss, rows, h->loss);
     // dW3 = dZ3^T H2, db3
     GemmArgs a = gemm_args(h->dz3, 0, 1, kOut, h->h2, 1, 1, kHid, kOut, kHid, rows, h->err);
     BMM_TRY(gemm_wgrad(a, h->g + kW3, h->part, s));
