@@ -150,6 +150,7 @@ SIGNATURES = {
     "bmm_gen_instance": [_u64p, _sz, _sz, _sz, C.c_double, C.c_uint64, _sz],
     "bmm_probe_xor_popc": [C.POINTER(C.c_double)],
     "bmm_gray_tune": [C.c_int, C.c_int],
+    "bmm_gray_tune_lanes": [C.c_int],
     "bmm_last_error": [],
     "bmm_version": [],
     "bmm_runtime_features": [C.POINTER(Features_t)],
@@ -213,7 +214,7 @@ SIGNATURES = {
     "bmm_matrix_load_binary": [C.c_char_p, _u64p, _sz, _sz, _sz],
     "bmm_matrix_load_binary_dev": [C.c_char_p, _vp, _sz, _sz, _sz, _vp],
     "bmm_matrix_hash": [_u64p, _sz, _sz, _sz, C.c_char_p],
-    "bmm_search_apply_dev": [_vp, _sz, _sz, _u32p, _sz, _sz, C.POINTER(SweepConfig_t),
+    "bmm_search_apply_dev": [_vp, _sz, _sz, _sz, _u32p, _sz, _sz, C.POINTER(SweepConfig_t),
                              C.POINTER(ApplyResult_t), _u64p, _vp],
     "bmm_sa_pairwise_table_dev": [_vp, _sz, _sz, _sz, _vp, _vp],
 }

@@ -677,7 +677,7 @@ int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) 
 }
 
 // Gradients of the mean cross-entropy for the forward pass just run (rows,
-// targets T [rows][256]) into h->g; the loss is added to *h->loss.
+// targets T [rows][256]) into h->g; the loss is written to *h->loss.
 int backward_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows) {
     cudaStream_t s = h->stream;
     xent_kernel<<<(rows * 32 + 255) / 256, 256, 0, s>>>(h->z3, T, h->dz3, h->row_loss, rows);

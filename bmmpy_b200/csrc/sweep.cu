@@ -34,6 +34,7 @@ struct WinState {
     unsigned long long applied, improvement;  // ApplyResult of the window
     int changed;                              // T != identity
     int error;                                // global applier: no full transform
+    int skipped;                              // not searched: an earlier window failed
 };
 
 // Window rows into a packed t x W block; row weights into the state.
@@ -69,9 +70,15 @@ struct Rng {
 __global__ void greedy_decide_kernel(const bmm_candidate* __restrict__ cands, int kk, int t,
                                      unsigned long long min_gain, int stochastic,
                                      unsigned long long* __restrict__ rng_state,
-                                     int* __restrict__ order, WinState* __restrict__ st) {
+                                     int* __restrict__ order, const int* __restrict__ abort_flag,
+                                     WinState* __restrict__ st) {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
+    if (*abort_flag) {  // an earlier window failed: the sweep stops there
+        st->skipped = 1;
+        st->changed = 0;
+        return;
+    }
     int n = 0;
     for (int i = 0; i < kk; ++i)
         if (cands[i].weight != 0xffffffffu)
@@ -156,11 +163,20 @@ __global__ void greedy_decide_kernel(const bmm_candidate* __restrict__ cands, in
 // GlobalGreedyApplier (src/apply/global_greedy_applier.cpp:30-91): candidates
 // and unit rows in one pool, stable-sorted by weight, inserted into a pivot
 // basis (pivot = highest set bit) until t are independent; T = the chosen
-// masks.  One thread; order[] is scratch for kk + t entries.
+// masks.  One thread; order[] is scratch for kk + t entries.  A window that
+// cannot assemble t independent masks sets *abort_flag, and every later window
+// of the call becomes a no-op, as the reference loop stops at the exception
+// (with the unit rows in the pool this cannot happen for valid candidates).
 __global__ void global_decide_kernel(const bmm_candidate* __restrict__ cands, int kk, int t,
-                                     int* __restrict__ order, WinState* __restrict__ st) {
+                                     int* __restrict__ order, int* __restrict__ abort_flag,
+                                     WinState* __restrict__ st) {
     if (threadIdx.x != 0 || blockIdx.x != 0)
         return;
+    if (*abort_flag) {
+        st->skipped = 1;
+        st->changed = 0;
+        return;
+    }
     int n = 0;
     for (int i = 0; i < kk; ++i)
         if (cands[i].weight != 0xffffffffu)
@@ -200,6 +216,8 @@ __global__ void global_decide_kernel(const bmm_candidate* __restrict__ cands, in
     }
     st->error = chosen != t;
     st->changed = chosen == t;
+    if (chosen != t)
+        *abort_flag = 1;
 }
 
 // rows_out[i] = XOR of rows_in[j] for j in T[i] (t x W, word-parallel).
@@ -262,7 +280,7 @@ using namespace bmm;
 
 extern "C" {
 
-BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
+BMM_API int bmm_search_apply_dev(uint64_t* words, size_t rows, size_t stride, size_t cols,
                                  const uint32_t* windows, size_t t, size_t n_windows,
                                  const bmm_sweep_config* cfg, bmm_apply_result* results,
                                  uint64_t* final_state, void* stream) {
@@ -286,9 +304,12 @@ BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
     const size_t kk = std::min<size_t>(cfg->max_candidates, states);
     if (kk > 1024)
         return fail(BMM_EINVAL, "search_apply: max_candidates above 1024 is not supported");
+    // every row index is checked here, before anything is launched: the
+    // kernels index the matrix with them unchecked
     for (size_t i = 0; i < n_windows * t; ++i)
-        if (windows[i] >= (uint32_t)0xffffffffu)
-            return fail(BMM_EINVAL, "search_apply: bad row index");
+        if ((size_t)windows[i] >= rows)
+            return fail(BMM_EINVAL, "search_apply: row index %u out of range (rows = %zu)",
+                        windows[i], rows);
     for (size_t q = 0; q < n_windows; ++q)
         for (size_t i = 0; i < t; ++i)
             for (size_t j = 0; j < i; ++j)
@@ -305,7 +326,8 @@ BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
     if (!ws)
         return st_;
     cudaStream_t s = (cudaStream_t)stream;
-    // scratch: window lists, packed rows (old, new), candidates, states, rng
+    // scratch: window lists, packed rows (old, new), candidates, states, rng,
+    // the sticky abort flag
     void *d_win = nullptr, *d_rows = nullptr, *d_new = nullptr, *d_cand = nullptr,
          *d_state = nullptr, *d_order = nullptr, *d_rng = nullptr;
     // (the spectrum search allocates its own slots; these are not among them)
@@ -314,12 +336,14 @@ BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
     BMM_TRY(ws_buffer(ws, kSlotSweepNew, t * W * 8, &d_new));
     BMM_TRY(ws_buffer(ws, kSlotOut, kk * sizeof(bmm_candidate), &d_cand));
     BMM_TRY(ws_buffer(ws, kSlotSweepState, n_windows * sizeof(sweep::WinState), &d_state));
-    BMM_TRY(ws_buffer(ws, kSlotSweepOrder, (kk + t) * sizeof(int) + 16, &d_order));
+    BMM_TRY(ws_buffer(ws, kSlotSweepOrder, (kk + t) * sizeof(int) + 32, &d_order));
     d_rng = (char*)d_order + (kk + t) * sizeof(int);
     d_rng = (void*)(((uintptr_t)d_rng + 7) & ~(uintptr_t)7);
+    int* d_abort = (int*)((char*)d_rng + 8);
     BMM_CUDA_TRY(cudaMemcpyAsync(d_win, windows, n_windows * t * 4, cudaMemcpyHostToDevice, s));
     BMM_CUDA_TRY(cudaMemcpyAsync(d_rng, &seed, 8, cudaMemcpyHostToDevice, s));
     BMM_CUDA_TRY(cudaMemsetAsync(d_state, 0, n_windows * sizeof(sweep::WinState), s));
+    BMM_CUDA_TRY(cudaMemsetAsync(d_abort, 0, sizeof(int), s));
     sweep::WinState* states_d = (sweep::WinState*)d_state;
     const unsigned gx = (unsigned)std::min<size_t>((W + 255) / 256, 64);
     const unsigned tb = (unsigned)std::min<size_t>((t * W + 255) / 256, (size_t)ws->sm_count * 4);
@@ -334,12 +358,12 @@ BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
         if (cfg->applier == 0) {
             sweep::greedy_decide_kernel<<<1, 32, 0, s>>>(
                 (const bmm_candidate*)d_cand, (int)kk, (int)t, cfg->min_gain,
-                cfg->stochastic ? 1 : 0, (unsigned long long*)d_rng, (int*)d_order, st);
+                cfg->stochastic ? 1 : 0, (unsigned long long*)d_rng, (int*)d_order, d_abort, st);
             sweep::transform_kernel<<<tb, 256, 0, s>>>((const uint64_t*)d_rows, (int)t, (int)W,
                                                        st, (uint64_t*)d_new, nullptr);
         } else {
             sweep::global_decide_kernel<<<1, 32, 0, s>>>((const bmm_candidate*)d_cand, (int)kk,
-                                                         (int)t, (int*)d_order, st);
+                                                         (int)t, (int*)d_order, d_abort, st);
             sweep::transform_kernel<<<tb, 256, 0, s>>>((const uint64_t*)d_rows, (int)t, (int)W,
                                                        st, (uint64_t*)d_new, &st->new_weight);
         }

@@ -108,7 +108,8 @@ class DeviceMatrix:
         res = (N.ApplyResult_t * max(1, n))()
         state = C.c_uint64(0)
         stream = torch.cuda.current_stream(self.device).cuda_stream
-        N.check(N.lib().bmm_search_apply_dev(self._words.data_ptr(), self.stride, self.cols,
+        N.check(N.lib().bmm_search_apply_dev(self._words.data_ptr(), self.rows, self.stride,
+                                             self.cols,
                                              N.u32p(wins), t, n, cfg, res, C.byref(state),
                                              stream), "bmm_search_apply_dev")
         if isinstance(applier, GreedyApplier) and applier.stochastic:

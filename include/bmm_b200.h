@@ -114,6 +114,10 @@ BMM_API uint64_t bmm_gen_instance(uint64_t* words, size_t rows, size_t cols, siz
  * prefix (-1 = built-in policy).  Process-wide; results never change, only
  * speed. */
 BMM_API int bmm_gray_tune(int hs_blocks, int chunk_bits);
+/* Lanes per prefix of the per-target Gray kernel for rows of 33-64 words:
+ * 1 (a lane holds the whole row) or 2 (a lane pair, 32 words each, more
+ * warps per SM); -1 = built-in policy.  Results never change, only speed. */
+BMM_API int bmm_gray_tune_lanes(int lanes);
 
 /* ---- batched per-target searches (thousands of uneven instances) ----
  * Instance i is a rows x cols matrix stored at words + word_offset with
@@ -227,7 +231,10 @@ BMM_API int bmm_gray_targets_dev(const uint64_t* d_words, size_t rows, size_t st
  * The first call on each device looks up that array's device address, so
  * make the first call on a device before any stream capture.  All calls
  * share the array: calls whose executions overlap on the GPU (different
- * streams, or different host threads) race; serialise them. */
+ * streams, or different host threads) race; serialise them.  The looked-up
+ * address is cached for the life of the process: a cudaDeviceReset between
+ * calls is not supported.  chunk_bits set by bmm_gray_tune applies here as it
+ * does to bmm_gray_targets_dev. */
 #define BMM_NOALLOC_MAX_TARGETS 16384
 BMM_API int bmm_gray_targets_noalloc(const uint64_t* d_words, size_t rows, size_t stride,
                                      size_t cols, const uint32_t* d_targets,
@@ -523,7 +530,10 @@ BMM_API int bmm_matrix_hash(const uint64_t* words, size_t stride, size_t rows, s
  * (0: GreedyApplier(min_gain, stochastic, seed) -- one generator carried from
  * window to window as one applier object would; 1: GlobalGreedyApplier(
  * require_improvement)) update the matrix rows in place.  windows: host array
- * of n_windows x t row indices.  results: one ApplyResult per window.
+ * of n_windows x t row indices, each < rows (checked on the host before any
+ * launch: BMM_EINVAL, where the reference raises IndexError).  results: one
+ * ApplyResult per window; when a window fails (BMM_ERUNTIME) the later
+ * windows of the call are left untouched, as the reference loop stops there.
  * cfg->seed is the greedy generator's state on entry (0 -> 0xDEADB, as the
  * constructor); final_state (optional) receives it on exit.  Synchronises
  * `stream` once, at the end. */
@@ -542,7 +552,7 @@ typedef struct bmm_apply_result {
     uint64_t weight_improvement;
 } bmm_apply_result;
 
-BMM_API int bmm_search_apply_dev(uint64_t* words, size_t stride, size_t cols,
+BMM_API int bmm_search_apply_dev(uint64_t* words, size_t rows, size_t stride, size_t cols,
                                  const uint32_t* windows, size_t t, size_t n_windows,
                                  const bmm_sweep_config* cfg, bmm_apply_result* results,
                                  uint64_t* final_state, void* stream);

@@ -95,3 +95,25 @@ def test_sweep_argument_errors():
     assert dev.search_apply(np.zeros((0, 4), np.uint32), searcher=bmm.MitmFwhtSearch(),
                             applier=bmm.GreedyApplier(1)) == []
     assert dev.to_matrix() == m
+
+
+def test_sweep_c_abi_rejects_out_of_range_rows():
+    # a C caller that skips the Python wrapper's IndexError check gets
+    # BMM_EINVAL from the library before anything is launched, and the
+    # matrix is untouched
+    import ctypes as C
+
+    from bmmpy_b200 import _native as N
+
+    m = _instance(20, 100, 0.2, 1, 0)
+    dev = bmm.DeviceMatrix(m)
+    wins = np.ascontiguousarray(np.array([[1, 2, 3], [4, 5, 20]], dtype=np.uint32))
+    cfg = N.SweepConfig_t()
+    cfg.max_candidates = 8
+    res = (N.ApplyResult_t * 2)()
+    state = C.c_uint64(0)
+    rc = N.lib().bmm_search_apply_dev(dev._words.data_ptr(), dev.rows, dev.stride, dev.cols,
+                                      N.u32p(wins), 3, 2, cfg, res, C.byref(state), 0)
+    assert rc == N.EINVAL
+    assert b"out of range" in N.lib().bmm_last_error()
+    assert dev.to_matrix() == m
