@@ -15,9 +15,11 @@ One step = all 40 targets = 40 * 2^24 = 671,088,640 row-combos.
   (bmmpy_b200.targets.gray_targets) from pinned host buffers: H2D of the
   matrix and index lists and D2H of the results inside the timed region.
 * ``roofline``: the dominant kernel (gray_targets_kernel) is bound by the
-  64-bit XOR+POPC issue rate, not by HBM (its rows live in shared memory) nor
-  by tensor cores; the peak is measured in this run by a register-only probe
-  kernel with the same per-word instruction mix (bmm_probe_xor_popc).
+  ALU and XU integer pipes (LOP3 XOR / carry-save adders and POPC), not by
+  HBM (its rows live in shared memory) nor by tensor cores; the peak is the
+  pipe bound of its instruction mix (counted by ncu) at the sampled SM clock.
+* The timed result is asserted equal to the reference's per-target answers
+  (tests/golden/workloads.npz) before the line is printed.
 * ``cpu_baseline``: the reference's BruteforceSearch (oracle/_ref, OpenMP on
   all host threads) on the 25-row window [i, others] for a bounded sample of
   targets; falls back to the oracle's C port when oracle/_ref is absent.
@@ -25,7 +27,10 @@ One step = all 40 targets = 40 * 2^24 = 671,088,640 row-combos.
 Multi-GPU: one process per GPU (torchrun); rank r runs the same workload on
 its own instance (seed 1 + r), no collective on the data path ("weak").
 ``--impl reference`` times the reference CPU implementation instead (rank 0
-only).
+only).  ``--impl reference-gpu`` times the reference's own CUDA searchers
+(CudaBruteforceSearch on the same 25-row windows, CudaMitmFwhtSearch on an
+int16-safe 32-row window) built for sm_100a, next to this library's classes of
+the same names on the same windows, and checks the results are equal.
 
 ``--workload basis`` (1 GPU) measures ExactBasisSolver on ten 24-row windows
 of the planted 256 x 8192 matrix: ``value`` from the device histogram pass on
@@ -157,17 +162,40 @@ def clock_summary(sampler):
             "reasons": sorted(reasons), "samples": len(sms)}
 
 
-def load_traffic():
-    """dram bytes per launch of gray_targets_kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "gray_targets_c2.md")
-    try:
-        with open(path) as f:
-            for ln in f:
-                if ln.startswith("dram_bytes_per_launch:"):
-                    return int(ln.split(":", 1)[1])
-    except (OSError, ValueError):
-        pass
-    return None
+# Roofline of gray_targets_kernel<64, 1, 4, 0> (the C2 step).  Its rows live
+# in shared memory and registers, so neither HBM nor tensor cores bound it:
+# each Gray step is 64 word XORs plus a popcount, split between LOP3 on the
+# ALU pipe (16 lanes per SM sub-partition: 2 cycles per warp instruction) and
+# POPC on the XU pipe (4 lanes: 8 cycles).  Warp instructions per warp-step
+# (32 lanes, one combo each, 64 words each) counted by ncu on this kernel
+# (smsp__inst_executed_pipe_{alu,xu}.sum and smsp__inst_executed.sum over one
+# C2 launch divided by its 40 * 2^24 / 32 warp-steps):
+GRAY_MIX = {"alu": 260, "xu": 72, "issue": 470}
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
+# same capture: the rows are read once into shared memory.
+GRAY_TRAFFIC = None
+
+
+def gray_pipe_bound(sm_count, mhz, mix=None, words=64):
+    """Words/s the SMs can process at the pipe bound of an instruction mix:
+    per sub-partition a warp-step takes max(2 * ALU, 8 * XU, issue) cycles."""
+    mix = mix or GRAY_MIX
+    cycles = max(2 * mix["alu"], 8 * mix["xu"], mix["issue"])
+    return sm_count * 4 * mhz * 1e6 * 32 * words / cycles
+
+
+def gray_best_mix_bound(sm_count, mhz, words=64, overhead_alu=10, overhead_xu=9):
+    """The same bound for the best split of a 64-word step between carry-save
+    LOP3 (2 per 32-bit word, ALU) and POPC (1 per 32-bit word, XU), with the
+    128 XOR LOP3 and the popcount sums on the FMA pipe: min over x of
+    max(2 * (128 + 256 x + oa), 8 * (128 (1 - x) + ox))."""
+    best = None
+    for i in range(0, 1001):
+        x = i / 1000
+        c = max(2 * (2 * words + 4 * words * x + overhead_alu),
+                8 * (2 * words * (1 - x) + overhead_xu))
+        best = c if best is None or c < best else best
+    return sm_count * 4 * mhz * 1e6 * 32 * words / best
 
 
 # ---------------------------------------------------------------------------
@@ -243,6 +271,101 @@ def run_reference(args, rank, world):
                                    if kind == "reference" else
                                    "one target per step: oracle C port Gray sweep (2^24 combos)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# The reference's own CUDA searchers on the same B200 (the GPU bar): the
+# unmodified reference built with its CUDA backend for sm_100a
+# (oracle/_ref/cuda, make -C oracle ref-cuda), called through its public
+# classes, next to this library's classes of the same names on the same
+# windows, results compared.
+MITM16 = dict(rows=32, cols=2048, p=0.2, seed=2)  # total weight ~13k: int16-safe
+
+
+def run_reference_gpu(args, rank, world):
+    if rank != 0:
+        return 0
+    from oracle.oracle import port, ref_cuda
+
+    RC = ref_cuda()
+    if RC is None:
+        print(json.dumps({"impl": "reference-gpu",
+                          "unavailable": "oracle/_ref/cuda was not built (make -C oracle "
+                                         "ref-cuda needs the reference checkout)"}))
+        return 0
+    import bmmpy_b200 as bmm
+    from bmmpy_b200.matrix import BitMatrix
+
+    P = port()
+    words, _ = P.gen_instance(ROWS, COLS, P_DENS, SEED)
+    m = BitMatrix.from_words(words, COLS)
+
+    def window(i):
+        i %= ROWS
+        return [i] + [(i + 1 + j) % ROWS for j in range(K_OTHERS)]
+
+    def timed(fn, steps):
+        out, per = None, []
+        for i in range(steps):
+            t0 = time.perf_counter()
+            out = fn(i)
+            per.append(time.perf_counter() - t0)
+        return out, per
+
+    # brute force: CudaBruteforceSearch(k=128) on the 25-row window [i, i+1..i+24]
+    ours = bmm.CudaBruteforceSearch(max_candidates=128)
+    ref_bf = lambda i: RC.cuda_bruteforce_search(words, COLS, window(i), 128)
+    our_bf = lambda i: [(c.mask_u64(), c.weight) for c in ours.search(m.row_window(window(i)))]
+    timed(ref_bf, args.warmup)
+    timed(our_bf, args.warmup)
+    want, ref_per = timed(ref_bf, args.steps)
+    got, our_per = timed(our_bf, args.steps)
+    assert got == want, "CudaBruteforceSearch results differ from the reference's"
+    combos = (1 << (K_OTHERS + 1)) - 1
+    ref_v = combos * len(ref_per) / sum(ref_per)
+    our_v = combos * len(our_per) / sum(our_per)
+
+    # meet-in-the-middle: CudaMitmFwhtSearch(k=64) on a 32-row window whose
+    # total weight fits the reference's int16 guard
+    mw, _ = P.gen_instance(MITM16["rows"], MITM16["cols"], MITM16["p"], MITM16["seed"])
+    mm = BitMatrix.from_words(mw, MITM16["cols"])
+    win = list(range(MITM16["rows"]))
+    t0 = time.perf_counter()
+    mwant = RC.cuda_mitm_search(mw, MITM16["cols"], win, 64)
+    ref_mitm_s = time.perf_counter() - t0
+    osearch = bmm.CudaMitmFwhtSearch(max_candidates=64)
+    osearch.search(mm.row_window(win))  # warm
+    t0 = time.perf_counter()
+    mgot = [(c.mask_u64(), c.weight) for c in osearch.search(mm.row_window(win))]
+    our_mitm_s = time.perf_counter() - t0
+    assert mgot == mwant, "CudaMitmFwhtSearch results differ from the reference's"
+
+    line = {
+        "impl": "reference-gpu", "metric": METRIC, "value": ref_v, "unit": UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * sum(ref_per) / len(ref_per), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "synthetic (xorshift64 seed 1)",
+        "config": {"workload": "reference CudaBruteforceSearch(k=128) on the 25-row windows "
+                               "[i, i+1..i+24] of the 40x4096 Bernoulli(0.3) matrix (seed 1), "
+                               "one window per step, 2^25-1 combos each",
+                   "kernel": "bruteforce_persistent_kernel<64> (reference, sm_100a)"},
+        "timing": "host wall clock around the synchronous public search() call "
+                  "(plan upload, kernels, result copy), both libraries alike",
+        "b200_same_call": {"value": our_v, "unit": UNIT,
+                           "ms_per_step": 1e3 * sum(our_per) / len(our_per),
+                           "ratio": our_v / ref_v, "results_equal": True},
+        "mitm": {"workload": f"CudaMitmFwhtSearch(k=64) on a {MITM16['rows']}x{MITM16['cols']} "
+                             f"Bernoulli({MITM16['p']}) window (seed {MITM16['seed']}), "
+                             "2^32 subsets, total weight within the reference's int16 guard",
+                 "reference_s": ref_mitm_s, "b200_s": our_mitm_s,
+                 "reference_combos_per_s": float(1 << 32) / ref_mitm_s,
+                 "b200_combos_per_s": float(1 << 32) / our_mitm_s,
+                 "ratio": ref_mitm_s / our_mitm_s, "results_equal": True},
+        "e2e": {"value": ref_v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -918,7 +1041,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa", "io", "mlp"])
     ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
@@ -948,6 +1071,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.impl == "reference-gpu":
+        return run_reference_gpu(args, rank, world)
 
     import torch
 
@@ -1013,8 +1138,14 @@ def main():
     combos_step = ROWS * COMBOS_PER_TARGET
     value = weak_throughput(world, combos_step * args.steps, max_ms / 1e3)
 
-    # correctness of what was timed: rank 0 instance == the golden answer
+    # correctness of what was timed: rank 0's instance (seed 1) is the C2
+    # workload, whose per-target answers the reference produced
     got_w = d_w.cpu().numpy().view(np.uint32)
+    got_m = d_mask.cpu().numpy().view(np.uint64)
+    if rank == 0:
+        gold = np.load(os.path.join(ROOT, "tests", "golden", "workloads.npz"))
+        assert np.array_equal(got_w, gold["c2_weight"]) and np.array_equal(
+            got_m, gold["c2_mask"]), "timed result differs from the reference's answer"
 
     # end to end through the public host API, pinned host inputs
     pinned = torch.empty(m.words.size, dtype=torch.int64, pin_memory=True).numpy()
@@ -1040,22 +1171,29 @@ def main():
     e2e_value = weak_throughput(world, combos_step * e_steps, max_over_ranks(e_dt, dist, dev))
     assert np.array_equal(ew, got_w), "e2e and resident results differ"
 
-    # roofline: XOR+POPC word rate of the targets kernel vs the measured probe
+    # roofline: 64-bit words XORed and counted per second by the targets
+    # kernel against the ALU/XU pipe bound of its instruction mix at the clock
+    # sampled during the timed region
     import ctypes
 
-    peak = ctypes.c_double(0)
-    N.check(N.lib().bmm_probe_xor_popc(ctypes.byref(peak)))
     per_launch_ms = max_ms / args.steps
     words = m.words_per_row
     achieved = combos_step * words / (per_launch_ms / 1e3)
-    traffic = load_traffic()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = gray_pipe_bound(sms, mhz)
+    probe = ctypes.c_double(0)
+    N.check(N.lib().bmm_probe_xor_popc(ctypes.byref(probe)))
     roofline = {
-        "bound": "int-popc",
-        "achieved": achieved / 1e9, "peak": peak.value / 1e9, "unit": "G words/s (64-bit XOR+POPC)",
-        "frac": achieved / peak.value,
-        "peak_source": "measured in this run: register-only XOR+POPC probe kernel "
-                       "(bmm_probe_xor_popc); not an HBM or tensor-core bound",
-        "traffic": traffic,
+        "bound": "alu+xu pipes",
+        "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G words/s (64-bit XOR+popcount)",
+        "frac": achieved / peak,
+        "peak_source": f"ALU/XU pipe bound of the kernel's instruction mix per warp-step "
+                       f"(ncu: {GRAY_MIX['alu']} ALU, {GRAY_MIX['xu']} XU, {GRAY_MIX['issue']} "
+                       f"issued) x {sms} SMs x {mhz:.0f} MHz sampled",
+        "frac_of_best_mix": achieved / gray_best_mix_bound(sms, mhz),
+        "xor_popc_probe": probe.value / 1e9,
+        "traffic": GRAY_TRAFFIC,
     }
 
     if dist:

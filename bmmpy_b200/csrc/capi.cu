@@ -284,6 +284,14 @@ int bmm_gray_tune(int hs_blocks, int chunk_bits) {
     return BMM_OK;
 }
 
+int bmm_gray_tune_lanes(int lanes) {
+    clear_error();
+    if (lanes != -1 && lanes != 1 && lanes != 2)
+        return fail(BMM_EINVAL, "gray tuning: lanes must be -1, 1 or 2");
+    g_gray_tuning.lanes = lanes;
+    return BMM_OK;
+}
+
 int bmm_probe_xor_popc(double* words_per_second) {
     clear_error();
     if (!words_per_second)
@@ -503,7 +511,7 @@ static int gray_targets_common(Workspace* ws, const uint64_t* d_words, size_t ro
             G *= 2;
         lanes = (int)G;
     }
-    int chunk = auto_chunk_bits((int)k, lanes, ws->sm_count, (int)n_targets);
+    int chunk = targets_chunk_bits((int)k, lanes, ws->sm_count, (int)n_targets);
     if (g_gray_tuning.chunk_bits > 0)
         chunk = g_gray_tuning.chunk_bits;
     if (chunk > (int)k)

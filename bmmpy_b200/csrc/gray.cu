@@ -69,14 +69,20 @@ __device__ __forceinline__ uint32_t group_sum(uint32_t v) {
     return v;
 }
 
-// Stage `nrows` rows (row r from src + idx(r) * stride, W words) into shared
-// memory as nrows x (G*WPL) words, zero padded.
+// Shared-memory row layout: a row is G lane slices of WPL words; with G > 1
+// each slice is followed by 2 pad words (16 bytes), so the G lanes of a group
+// read their slices' 16-byte chunks from different banks in one request.
+__host__ __device__ constexpr int lane_stride(int wpl, int g) { return wpl + (g > 1 ? 2 : 0); }
+__host__ __device__ constexpr int row_stride(int wpl, int g) { return g * lane_stride(wpl, g); }
+
+// Stage `nrows` rows (row r from row_of(r), W words) into shared memory in
+// that layout (row stride row_stride(WPL, G) words), zero padded past W.
 template <int WPL, int G, typename RowOf>
 __device__ __forceinline__ void stage_rows(uint64_t* srow, int nrows, int W, RowOf row_of) {
-    constexpr int SW = WPL * G;
-    for (int i = threadIdx.x; i < nrows * SW; i += blockDim.x) {
-        const int r = i / SW, w = i % SW;
-        srow[i] = w < W ? row_of(r)[w] : 0ull;
+    constexpr int RW = WPL * G, LS = lane_stride(WPL, G), SW = row_stride(WPL, G);
+    for (int i = threadIdx.x; i < nrows * RW; i += blockDim.x) {
+        const int r = i / RW, w = i % RW;
+        srow[r * SW + (w / WPL) * LS + w % WPL] = w < W ? row_of(r)[w] : 0ull;
     }
 }
 
@@ -88,7 +94,7 @@ __global__ void __launch_bounds__(kThreads)
     gray_window_kernel(const uint64_t* __restrict__ rows, int t, int W, int chunk,
                        unsigned long long n_prefix, int kk, bmm_candidate* __restrict__ cta_out) {
     extern __shared__ __align__(16) uint64_t srow[];
-    constexpr int SW = WPL * G;
+    constexpr int SW = row_stride(WPL, G);
     stage_rows<WPL, G>(srow, t, W, [&](int r) { return rows + (size_t)r * W; });
     __syncthreads();
 
@@ -104,7 +110,7 @@ __global__ void __launch_bounds__(kThreads)
     top.init();
     uint32_t thr = 0xffffffffu;
 
-    const uint64_t* my = srow + gl * WPL;
+    const uint64_t* my = srow + gl * lane_stride(WPL, G);
     while (__any_sync(kFull, p < n_prefix)) {
         const bool valid = p < n_prefix && gl == 0;
         uint64_t cur[WPL];
@@ -148,15 +154,31 @@ __global__ void __launch_bounds__(kThreads)
 
 // ---------------------------------------------------------------------------
 // Per-target top-1.  CTA b serves target b / ctas_per_target.
-// key = (weight << 40) | tie, tie = S (tiebreak 0) or inverse-Gray(S).
-template <int WPL, int G, int NHB>
-__global__ void __launch_bounds__(kThreads)
+// key = (weight << 40) | tie, tie = S (TB 0) or inverse-Gray(S) (TB 1).
+// Within a lane's walk the prefix part of the tie is fixed, so the running
+// best is one 32-bit key (weight << chunk) | low tie bits, built by an IMAD
+// (weight * wmul + tie, wmul = one << chunk) and kept by one integer min;
+// the host keeps chunk + bits(max weight) <= 32.  `one` is 1 at run time.
+// Carry-save blocks per step of the per-target kernel.  With its popcount
+// sums on the FMA pipe, 4 of the 8 blocks of a 64-word lane balance the ALU
+// (XOR + carry-save LOP3) and XU (POPC) pipes best: 40 x 4096, k = 24 on
+// B200 takes 13.5 ms with 4 blocks, 14.0 ms with 5, 14.7 ms with 3.
+constexpr int targets_nhb(int wpl) { return wpl >= 64 ? 4 : default_nhb(wpl); }
+
+// CTAs per SM the register budget is set for.  64-word lanes: no minimum;
+// the compiler's 234-register schedule (2 CTAs per SM) ran 8 % faster than a
+// 3-CTA budget (168 registers) and 28 % faster than an unrolled pair of steps.
+// 32-word lane pairs fit 6 CTAs in 80 registers without spills.
+constexpr int targets_min_ctas(int wpl) { return wpl == 32 ? 6 : 1; }
+
+template <int WPL, int G, int NHB, int TB>
+__global__ void __launch_bounds__(kThreads, targets_min_ctas(WPL))
     gray_targets_kernel(const uint64_t* __restrict__ words, int stride, int W,
                         const uint32_t* __restrict__ targets, const uint32_t* __restrict__ others,
-                        int k, int chunk, int tiebreak, int ctas_per_target,
+                        int k, int chunk, int ctas_per_target, uint32_t one,
                         unsigned long long* __restrict__ best_keys) {
     extern __shared__ __align__(16) uint64_t srow[];
-    constexpr int SW = WPL * G;
+    constexpr int SW = row_stride(WPL, G);
     const int ti = blockIdx.x / ctas_per_target;
     const int part = blockIdx.x % ctas_per_target;
     const uint32_t* oth = others + (size_t)ti * k;
@@ -173,7 +195,7 @@ __global__ void __launch_bounds__(kThreads)
     const unsigned long long n_prefix = 1ull << hb;
     const unsigned long long p = (unsigned long long)part * (kThreads / G) + threadIdx.x / G;
     const bool valid = p < n_prefix && gl == 0;
-    const uint64_t* my = srow + gl * WPL;
+    const uint64_t* my = srow + gl * lane_stride(WPL, G);
 
     uint64_t cur[WPL];
     {
@@ -189,29 +211,25 @@ __global__ void __launch_bounds__(kThreads)
         if ((p >> b) & 1ull)
             xor_row<WPL>(cur, my + (size_t)(chunk + b) * SW);
 
-    const uint64_t lowmask = (1ull << chunk) - 1;
-    const uint64_t hi_mask = p << chunk;
-    // tie key for the Gray order: inverse-Gray(S) = (ig(p) << chunk) | (s ^ flip)
-    const uint64_t hi_tie = tiebreak ? (inverse_gray64(p) << chunk) : hi_mask;
-    const uint64_t flip = (tiebreak && (__popcll(p) & 1)) ? lowmask : 0ull;
-
-    uint32_t best_w = group_sum<G>(popc_row<WPL>(cur));
-    uint64_t best_tie = tiebreak ? (hi_tie | flip) : hi_mask;
-    uint64_t low = 0;
+    const uint32_t lowmask = (uint32_t)((1ull << chunk) - 1);
+    // tie key in the Gray order: inverse-Gray(S) = (ig(p) << chunk) | (s ^ flip)
+    const uint32_t flip = (TB && (__popcll(p) & 1)) ? lowmask : 0u;
+    const uint32_t wmul = one << chunk;
     const uint32_t states = 1u << chunk;
+
+    uint32_t low = 0;  // low chunk bits of S (the Gray code of s)
+    uint32_t best = mad_u32(group_sum<G>(popc_row<WPL>(cur)), wmul, TB ? flip : 0u);
     for (uint32_t s = 1; s < states; ++s) {
         const int b = __ffs(s) - 1;
-        const uint32_t w = group_sum<G>(xor_row_popc_hs<WPL, NHB>(cur, my + (size_t)b * SW));
-        low ^= 1ull << b;
-        if (w <= best_w) {
-            const uint64_t tie = tiebreak ? (hi_tie | (s ^ flip)) : (hi_mask | low);
-            if (w < best_w || tie < best_tie) {
-                best_w = w;
-                best_tie = tie;
-            }
-        }
+        const uint32_t w =
+            group_sum<G>(xor_row_popc_hs_fma<WPL, NHB>(cur, my + (size_t)b * SW, one));
+        low ^= 1u << b;
+        best = min(best, mad_u32(w, wmul, TB ? (s ^ flip) : low));
     }
-    unsigned long long key = valid ? (((unsigned long long)best_w << 40) | best_tie) : ~0ull;
+    const uint64_t hi_tie = TB ? (inverse_gray64(p) << chunk) : (p << chunk);
+    const uint64_t best_w = chunk < 32 ? (best >> chunk) : 0;
+    unsigned long long key =
+        valid ? ((best_w << 40) | hi_tie | (uint64_t)(best & lowmask)) : ~0ull;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         const unsigned long long other = __shfl_xor_sync(kFull, key, o);
@@ -238,10 +256,11 @@ __global__ void decode_keys_kernel(const unsigned long long* __restrict__ keys, 
 // ---------------------------------------------------------------------------
 // host side
 
-// Carry-save blocks (of 8 words) per Gray step by lane width.  Without them
-// the XU pipe (POPC) saturates while ALU idles at ~36 %; 5 of the 8 blocks of
-// a 64-word lane through the adder tree measured fastest on B200 (40 x 4096,
-// k = 24: 20.3 ms -> 15.7 ms per step); narrower lanes keep the same ratio.
+// Carry-save blocks (of 8 words) per Gray step of the window kernel, by lane
+// width (default_nhb): without them the XU pipe (POPC) saturates while ALU
+// idles at ~36 %; 5 of the 8 blocks of a 64-word lane balanced the pipes when
+// the popcount sums were ALU adds (the per-target kernel, whose sums are
+// IMADs, uses 4: targets_nhb).
 
 int group_shape(size_t W, int* wpl, int* g) {
     if (W <= 2) {
@@ -267,6 +286,16 @@ int group_shape(size_t W, int* wpl, int* g) {
     return BMM_OK;
 }
 
+// The per-target kernel may split a 33-64-word row over a lane pair (32 words
+// each): half the registers per lane, so more warps fit per SM, for one
+// shuffle-add per step.
+int targets_shape(size_t W, int* wpl, int* g) {
+    BMM_TRY(group_shape(W, wpl, g));
+    if (*wpl == 64 && *g == 1 && W > 32 && g_gray_tuning.lanes == 2)
+        *wpl = 32, *g = 2;
+    return BMM_OK;
+}
+
 template <typename F>
 int dispatch_wg(int wpl, int g, F&& f) {
 #define BMM_WG(A, B)                                                                              \
@@ -277,6 +306,7 @@ int dispatch_wg(int wpl, int g, F&& f) {
     BMM_WG(8, 1)
     BMM_WG(16, 1)
     BMM_WG(32, 1)
+    BMM_WG(32, 2)
     BMM_WG(64, 1)
     BMM_WG(64, 2)
     BMM_WG(64, 4)
@@ -322,11 +352,30 @@ int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items) {
     return chunk;
 }
 
+int targets_chunk_bits(int k, int lanes_per_prefix, int sm_count, int n_targets) {
+    // The per-target kernel runs 2 CTAs per SM (234 registers: the schedule
+    // the compiler picks at that budget beat 3 CTAs per SM by 8 %); aim for
+    // enough prefixes to fill ~16 waves, but walk at least 2^10 Gray steps per
+    // prefix so the prefix set-up (up to k - chunk row XORs) stays near 1 %.
+    // Measured on 40 x 4096, k = 24: chunk 10 takes 13.49 ms, chunk 8 13.60.
+    const double want =
+        (double)sm_count * 2 * 16 * kThreads / lanes_per_prefix / (n_targets ? n_targets : 1);
+    int hb = 0;
+    while (hb < k && (double)(1ull << hb) < want)
+        ++hb;
+    int chunk = k - hb;
+    if (chunk < 10)
+        chunk = k < 10 ? k : 10;
+    if (chunk > 20)
+        chunk = 20;
+    return chunk > k ? k : chunk;
+}
+
 int gray_window_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, int chunk, int kk,
                        bmm_candidate* d_out, cudaStream_t stream) {
     int wpl = 0, g = 0;
     BMM_TRY(group_shape((size_t)W, &wpl, &g));
-    const size_t srow_bytes = (size_t)t * wpl * g * 8;
+    const size_t srow_bytes = (size_t)t * row_stride(wpl, g) * 8;
     const unsigned long long n_prefix = 1ull << (t - chunk);
     return dispatch_wg(wpl, g, [&](auto WPLc, auto Gc) -> int {
         constexpr int WPL = decltype(WPLc)::value, G = decltype(Gc)::value;
@@ -365,42 +414,67 @@ int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int 
                         int tiebreak, int chunk, unsigned long long* d_keys, uint64_t* d_best_mask,
                         uint32_t* d_best_weight, cudaStream_t stream) {
     int wpl = 0, g = 0;
-    BMM_TRY(group_shape((size_t)W, &wpl, &g));
-    const size_t smem = (size_t)(k + 1) * wpl * g * 8;
+    BMM_TRY(targets_shape((size_t)W, &wpl, &g));
+    const size_t smem = (size_t)(k + 1) * row_stride(wpl, g) * 8;
     if (smem > (size_t)ws->smem_optin)
         return fail(BMM_EINVAL, "gray targets: %zu bytes of rows exceed shared memory", smem);
+    // the kernel's running key is (weight << chunk) | low tie in 32 bits:
+    // chunk + bits(largest weight of a wpl * g-word row) <= 32 (speed only)
+    {
+        int wbits = 0;
+        while ((1ull << wbits) <= (unsigned long long)wpl * g * 64)
+            ++wbits;
+        if (chunk > 32 - wbits)
+            chunk = 32 - wbits;
+    }
     const unsigned long long n_prefix = 1ull << (k - chunk);
     const unsigned long long per_cta = kThreads / g;
     const unsigned long long ctas = (n_prefix + per_cta - 1) / per_cta;
     if (ctas * (unsigned long long)n_targets > 0x7fffffffull)
         return fail(BMM_EINVAL, "gray targets: grid too large (raise chunk_bits)");
     BMM_CUDA_TRY(cudaMemsetAsync(d_keys, 0xff, sizeof(unsigned long long) * n_targets, stream));
+    const uint32_t one = 1;
     BMM_TRY(dispatch_wg(wpl, g, [&](auto WPLc, auto Gc) -> int {
         constexpr int WPL = decltype(WPLc)::value, G = decltype(Gc)::value;
         auto go = [&](auto kern) -> int {
             BMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                               (int)smem));
             kern<<<(unsigned)(ctas * n_targets), kThreads, smem, stream>>>(
-                d_words, stride, W, d_targets, d_others, k, chunk, tiebreak, (int)ctas, d_keys);
+                d_words, stride, W, d_targets, d_others, k, chunk, (int)ctas, one, d_keys);
             BMM_CUDA_TRY(cudaGetLastError());
             return BMM_OK;
+        };
+        auto by_tb = [&](auto NHBc) -> int {
+            constexpr int NHB = decltype(NHBc)::value;
+            return tiebreak ? go(gray_targets_kernel<WPL, G, NHB, 1>)
+                            : go(gray_targets_kernel<WPL, G, NHB, 0>);
         };
         const int hs = g_gray_tuning.hs_blocks;
         if constexpr (WPL == 64 && G == 1) {
             switch (hs) {
             case -1: break;
-            case 0: return go(gray_targets_kernel<WPL, G, 0>);
-            case 2: return go(gray_targets_kernel<WPL, G, 2>);
-            case 3: return go(gray_targets_kernel<WPL, G, 3>);
-            case 4: return go(gray_targets_kernel<WPL, G, 4>);
-            case 5: return go(gray_targets_kernel<WPL, G, 5>);
-            case 6: return go(gray_targets_kernel<WPL, G, 6>);
-            case 8: return go(gray_targets_kernel<WPL, G, 8>);
+            case 0: return by_tb(std::integral_constant<int, 0>{});
+            case 2: return by_tb(std::integral_constant<int, 2>{});
+            case 3: return by_tb(std::integral_constant<int, 3>{});
+            case 4: return by_tb(std::integral_constant<int, 4>{});
+            case 5: return by_tb(std::integral_constant<int, 5>{});
+            case 6: return by_tb(std::integral_constant<int, 6>{});
+            case 8: return by_tb(std::integral_constant<int, 8>{});
             default: return fail(BMM_EINVAL, "gray tuning: hs_blocks must be 0, 2-6 or 8");
             }
         }
+        if constexpr (WPL == 32) {
+            switch (hs) {
+            case -1: break;
+            case 0: return by_tb(std::integral_constant<int, 0>{});
+            case 2: return by_tb(std::integral_constant<int, 2>{});
+            case 3: return by_tb(std::integral_constant<int, 3>{});
+            case 4: return by_tb(std::integral_constant<int, 4>{});
+            default: return fail(BMM_EINVAL, "gray tuning: hs_blocks must be 0, 2-4 for 32-word lanes");
+            }
+        }
         (void)hs;
-        return go(gray_targets_kernel<WPL, G, default_nhb(WPL)>);
+        return by_tb(std::integral_constant<int, targets_nhb(WPL)>{});
     }));
     decode_keys_kernel<<<(n_targets + 127) / 128, 128, 0, stream>>>(d_keys, n_targets, tiebreak,
                                                                     d_best_mask, d_best_weight);
@@ -559,7 +633,9 @@ extern "C" BMM_API int bmm_gray_targets_noalloc(const uint64_t* d_words, size_t 
     int lanes = 1;
     while ((size_t)lanes * 64 < W)
         lanes *= 2;
-    int chunk = auto_chunk_bits((int)k, lanes, d->sm_count, (int)n_targets);
+    int chunk = targets_chunk_bits((int)k, lanes, d->sm_count, (int)n_targets);
+    if (g_gray_tuning.chunk_bits > 0)  // the same tuning bmm_gray_targets_dev honours
+        chunk = g_gray_tuning.chunk_bits;
     if (chunk > (int)k)
         chunk = (int)k;
     // gray_targets_launch clears the keys it uses to ~0 before the search, so

@@ -10,11 +10,14 @@ namespace bmm {
 struct GrayTuning {
     int hs_blocks = -1;   // carry-save blocks per 64-word lane (0, 2-6, 8)
     int chunk_bits = -1;  // Gray-swept low bits per prefix
+    int lanes = -1;       // lanes per prefix for rows of 33-64 words (1 or 2)
 };
 extern GrayTuning g_gray_tuning;
 
 // Low chunk width giving enough independent prefixes to fill the device.
 int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items);
+// The same for the per-target kernel (its occupancy and walk length).
+int targets_chunk_bits(int k, int lanes_per_prefix, int sm_count, int n_targets);
 
 // Top-kk over all nonzero masks of the t rows in d_rows (t x W words).
 // d_out receives kk entries (empty ones have weight 0xffffffff).

@@ -93,3 +93,48 @@ def test_c4_first_instances(wl):
         assert np.array_equal(got, first[row:row + m.rows])
         assert checksum_pairs(fm, fw) == int(wl["c4_checksums"][idx])
         row += m.rows
+
+
+@pytest.mark.parametrize("lanes", [1, 2])
+@pytest.mark.parametrize("tiebreak", ["mask", "gray"])
+def test_gray_targets_lane_shapes_match_oracle(lanes, tiebreak):
+    """Rows of 33-64 words on one lane or a lane pair, and wider rows split
+    over 2-8 lanes (padded shared-memory slices), with carry-save variants."""
+    from bmmpy_b200 import _native as N
+
+    P = port()
+    rng = random.Random(17 + lanes)
+    L = N.lib()
+    try:
+        N.check(L.bmm_gray_tune_lanes(lanes))
+        for trial, cols in enumerate([2049, 3000, 4096, 4100, 9000, 20000]):
+            rows = rng.randint(14, 24)
+            words, _ = P.gen_instance(rows, cols, rng.choice([0.01, 0.3, 0.5]), 300 + trial)
+            k = rng.randint(6, min(rows - 1, 11))
+            m = BitMatrix.from_words(words, cols)
+            t, o = T.cyclic_others(rows, k, offset=rng.randint(1, rows - k))
+            for hs in ([-1, 0, 2, 4] if 2048 < cols <= 4096 else [-1]):
+                N.check(L.bmm_gray_tune(hs, rng.choice([-1, 3, 5])))
+                gm, gw = T.gray_targets(m, t, o, tiebreak=tiebreak)
+                for i in range(rows):
+                    exp = P.target_best_gray(words, cols, int(t[i]), o[i].tolist(),
+                                             1 if tiebreak == "gray" else 0)
+                    assert (int(gm[i]), int(gw[i])) == exp, (cols, hs, i)
+    finally:
+        N.check(L.bmm_gray_tune(-1, -1))
+        N.check(L.bmm_gray_tune_lanes(-1))
+
+
+def test_c2_full_size_lane_pairs(wl):
+    """The full C2 workload with 32-word lane pairs, bit-exact."""
+    from bmmpy_b200 import _native as N
+
+    L = N.lib()
+    m, _ = gen_instance(C2["rows"], C2["cols"], C2["p"], C2["seed"])
+    t, o = T.cyclic_others(C2["rows"], C2["k"])
+    try:
+        N.check(L.bmm_gray_tune_lanes(2))
+        gm, gw = T.gray_targets(m, t, o)
+    finally:
+        N.check(L.bmm_gray_tune_lanes(-1))
+    assert np.array_equal(gm, wl["c2_mask"]) and np.array_equal(gw, wl["c2_weight"])
