@@ -5,6 +5,9 @@
 * :func:`ref` -- the unmodified reference C++ library compiled from its own
   sources by ``make -C oracle ref`` (``oracle/_ref/libbmmref.so``); ``None``
   where it was not built.
+* :func:`ref_cuda` -- the same with the reference's CUDA backend
+  (``make -C oracle ref-cuda``): CudaBruteforceSearch and CudaMitmFwhtSearch
+  running the reference's own kernels; ``None`` where it was not built.
 
 Only the tests, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py``
 import this module; the product never does.  Matrices are numpy ``uint64``
@@ -26,6 +29,10 @@ REF_SO = os.path.join(HERE, "_ref", "libbmmref.so")
 # which the AVX2 build crashes on for rows of 4+ words: aligned loads in
 # src/core/bit_ops_avx2.cpp:21-24 on an unaligned std::vector)
 REF_SCALAR_SO = os.path.join(HERE, "_ref", "libbmmref_scalar.so")
+# the reference with its CUDA backend (its own GPU kernels, built for sm_100a
+# by ``make -C oracle ref-cuda``): the GPU bar bench.py's reference-gpu arm
+# times on the same B200
+REF_CUDA_SO = os.path.join(HERE, "_ref", "cuda", "libbmmref_cuda.so")
 
 _u64p = C.POINTER(C.c_uint64)
 _u32p = C.POINTER(C.c_uint32)
@@ -653,3 +660,47 @@ def ref_scalar():
     if _ref_scalar is None and os.path.exists(REF_SCALAR_SO):
         _ref_scalar = Ref(C.CDLL(REF_SCALAR_SO))
     return _ref_scalar
+
+
+class RefCuda:
+    """The reference's GPU searchers (oracle/_ref/cuda/libbmmref_cuda.so):
+    CudaBruteforceSearch / CudaMitmFwhtSearch on a window of a packed
+    matrix, through the reference's own classes and kernels."""
+
+    def __init__(self, lib):
+        self.lib = lib
+        for name in ("refc_cuda_bruteforce_search", "refc_cuda_mitm_search"):
+            fn = getattr(lib, name)
+            fn.restype = C.c_long
+            fn.argtypes = [_u64p, _sz, _sz, _sz, _szp, _sz, _sz, _sz, _u64p, _u32p, _sz]
+        lib.refc_last_error.restype = C.c_char_p
+
+    def _call(self, fn, m, cols, win, k, extra):
+        m = np.ascontiguousarray(m, dtype=np.uint64)
+        win = np.ascontiguousarray(win, dtype=np.uintp)
+        cap = max(int(k), 1)
+        masks = np.zeros(cap, np.uint64)
+        weights = np.zeros(cap, np.uint32)
+        n = fn(_ptr(m, _u64p), m.shape[0], cols, m.shape[1], _ptr(win, _szp), len(win), k, extra,
+               _ptr(masks, _u64p), _ptr(weights, _u32p), cap)
+        if n < 0:
+            raise ERRORS.get(n, OracleError)(self.lib.refc_last_error().decode())
+        n = min(n, cap)
+        return list(zip(masks[:n].tolist(), weights[:n].tolist()))
+
+    def cuda_bruteforce_search(self, m, cols, win, k=128, chunk_bits=0):
+        return self._call(self.lib.refc_cuda_bruteforce_search, m, cols, win, k, chunk_bits)
+
+    def cuda_mitm_search(self, m, cols, win, k=64, low_bits=0):
+        return self._call(self.lib.refc_cuda_mitm_search, m, cols, win, k, low_bits)
+
+
+_ref_cuda = None
+
+
+def ref_cuda():
+    """The reference's CUDA searchers, or None where they were not built."""
+    global _ref_cuda
+    if _ref_cuda is None and os.path.exists(REF_CUDA_SO):
+        _ref_cuda = RefCuda(C.CDLL(REF_CUDA_SO))
+    return _ref_cuda
