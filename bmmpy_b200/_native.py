@@ -151,6 +151,10 @@ SIGNATURES = {
     "bmm_probe_xor_popc": [C.POINTER(C.c_double)],
     "bmm_gray_tune": [C.c_int, C.c_int],
     "bmm_gray_tune_lanes": [C.c_int],
+    "bmm_spectrum_tune": [C.c_int],
+    "bmm_spectrum_low_bits": [_sz],
+    "bmm_spectrum_topk_slices_dev": [_vp, _sz, _sz, _sz, _sz, C.c_int, C.c_int64, C.c_int64, _vp,
+                                     _vp],
     "bmm_last_error": [],
     "bmm_version": [],
     "bmm_runtime_features": [C.POINTER(Features_t)],

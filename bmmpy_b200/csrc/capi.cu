@@ -625,3 +625,39 @@ int bmm_fwht_targets(const uint64_t* words, size_t rows, size_t stride, size_t c
 }
 
 }  // extern "C"
+
+// ---- spectrum slices (multi-GPU partition of one window's masks) ----------
+int bmm_spectrum_tune(int low_bits) {
+    clear_error();
+    if (low_bits != -1 && (low_bits < 14 || low_bits > 33))
+        return fail(BMM_EINVAL, "spectrum tuning: low_bits must be -1 or in [14, 33]");
+    g_spectrum_low_bits = low_bits;
+    return BMM_OK;
+}
+
+int bmm_spectrum_low_bits(size_t t) { return t > 40 ? -1 : spectrum_low_bits((int)t); }
+
+int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols, size_t k,
+                                 int low_bits, int64_t slice_begin, int64_t slice_end,
+                                 bmm_candidate* d_out, void* stream) {
+    clear_error();
+    if (t == 0 || t > 40)
+        return fail(BMM_EINVAL, "spectrum slices: t must be in [1, 40]");
+    if (!d_rows || !d_out)
+        return fail(BMM_EINVAL, "spectrum slices: null argument");
+    if (W < (cols + 63) / 64 || W == 0)
+        return fail(BMM_EINVAL, "spectrum slices: W smaller than the row width");
+    if (cols > 0x7fffffffull)
+        return fail(BMM_EOVERFLOW, "spectrum slices: total weight exceeds int32 range");
+    const size_t states = ((size_t)1 << t) - 1;
+    const size_t kk = k < states ? k : states;
+    if (kk == 0 || kk > 1024)
+        return fail(BMM_EINVAL, "spectrum slices: k must be in [1, 1024]");
+    int st = 0;
+    Workspace* ws = workspace(&st);
+    if (!ws)
+        return st;
+    return spectrum_topk_slices(ws, d_rows, (int)t, (int)W, (long long)cols, (int)kk, low_bits,
+                                (long long)slice_begin, (long long)slice_end, d_out,
+                                (cudaStream_t)stream);
+}

@@ -540,12 +540,36 @@ int grid_for(Workspace* ws, long long ntiles) {
 
 }  // namespace
 
+int g_spectrum_low_bits = -1;
+
+int spectrum_low_bits(int t) {
+    const int top = t < 33 ? t : 33;
+    if (g_spectrum_low_bits > 0 && t > kTileLog)
+        return g_spectrum_low_bits < kTileLog ? kTileLog
+                                              : (g_spectrum_low_bits > top ? top : g_spectrum_low_bits);
+    return top;
+}
+
 int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, long long cols,
                          int kk, bmm_candidate* d_out, cudaStream_t stream) {
+    return spectrum_topk_slices(ws, d_rows, t, W, cols, kk, -1, 0, -1, d_out, stream);
+}
+
+int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, long long cols,
+                         int kk, int low_bits, long long slice_begin, long long slice_end,
+                         bmm_candidate* d_out, cudaStream_t stream) {
     if (t < 1 || t > 40)
         return fail(BMM_EINVAL, "spectrum search: t must be in [1, 40]");
-    const int T = t < 33 ? t : 33;
+    const int T = low_bits < 0 ? spectrum_low_bits(t) : low_bits;
+    if (T > (t < 33 ? t : 33) || (T < kTileLog && T != t))
+        return fail(BMM_EINVAL, "spectrum search: low_bits must be in [14, min(t, 33)]");
     const int H = t - T;
+    const long long all_slices = 1ll << H;
+    if (slice_end < 0)
+        slice_end = all_slices;
+    if (slice_begin < 0 || slice_begin >= slice_end || slice_end > all_slices)
+        return fail(BMM_EINVAL, "spectrum search: slice range [%lld, %lld) outside [0, %lld)",
+                    slice_begin, slice_end, all_slices);
     void *pats = nullptr, *cnt = nullptr;
     BMM_TRY(ws_buffer(ws, kSlotAux, (size_t)(cols > 0 ? cols : 1) * 8, &pats));
     BMM_TRY(ws_buffer(ws, kSlotCounter, 16, &cnt));
@@ -600,7 +624,7 @@ int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
     // the double-buffered last middle pass: one persistent CTA per SM
     const int grid_last =
         nmid ? (int)std::min<long long>(ntiles, (long long)ws->sm_count) : grid_a;
-    const long long slices = 1ll << H;
+    const long long slices = slice_end - slice_begin;
     bmm_candidate *lists = nullptr, *slice_lists = nullptr;
     BMM_TRY(ws_buffer(ws, kSlotCand, (size_t)grid_last * kk * sizeof(bmm_candidate),
                       (void**)&lists));
@@ -610,8 +634,9 @@ int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
     const size_t smem = kTile * sizeof(int32_t);
     return dispatch_e(kk, [&](auto Ec) -> int {
         constexpr int E = decltype(Ec)::value;
-        for (long long x = 0; x < slices; ++x) {
-            bmm_candidate* dst = slices > 1 ? slice_lists + (size_t)x * kk : d_out;
+        for (long long x = slice_begin; x < slice_end; ++x) {
+            bmm_candidate* dst =
+                slices > 1 ? slice_lists + (size_t)(x - slice_begin) * kk : d_out;
             if (nmid == 0) {
                 auto k = pass_a_kernel<true, true, E>;
                 const size_t lsmem = pass_smem(true, E);

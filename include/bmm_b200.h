@@ -557,6 +557,26 @@ BMM_API int bmm_search_apply_dev(uint64_t* words, size_t rows, size_t stride, si
                                  const bmm_sweep_config* cfg, bmm_apply_result* results,
                                  uint64_t* final_state, void* stream);
 
+/* ---- spectrum slices: one window's masks split across devices ----------
+ * No reference counterpart (the reference searches a window on one device).
+ * The t-bit masks of a window split into low_bits low bits, materialised as
+ * one 2^low_bits spectrum per slice, and t - low_bits high bits, the slice
+ * index x.  bmm_spectrum_topk_slices_dev writes to d_out (device, k entries,
+ * empty ones with weight 0xffffffff) the k smallest (weight, mask) over the
+ * nonzero masks whose slice lies in [slice_begin, slice_end), of the t rows
+ * d_rows (device, t x W words, W >= ceil(cols / 64), bits past cols zero);
+ * asynchronous on `stream`.  Ranks that take disjoint slice ranges covering
+ * [0, 2^(t - low_bits)) and merge their lists by (weight, mask) get exactly
+ * the window's MitmFwhtSearch / FwhtSearch result.  low_bits = -1 uses
+ * bmm_spectrum_low_bits(t); otherwise 14 <= low_bits <= min(t, 33).
+ * bmm_spectrum_tune sets the default split (-1: min(t, 33)); results never
+ * change, only speed and memory (2^low_bits int32 per call). */
+BMM_API int bmm_spectrum_tune(int low_bits);
+BMM_API int bmm_spectrum_low_bits(size_t t);
+BMM_API int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols,
+                                         size_t k, int low_bits, int64_t slice_begin,
+                                         int64_t slice_end, bmm_candidate* d_out, void* stream);
+
 /* Autotuner hook for the enumeration kernel (no reference counterpart):
  * carry-save blocks of 8 words per 64-word lane (0, 2, 5 or 8; -1 = built-in
  * policy).  Process-wide; results never change, only speed. */
