@@ -170,10 +170,10 @@ def clock_summary(sampler):
 # (32 lanes, one combo each, 64 words each) counted by ncu on this kernel
 # (smsp__inst_executed_pipe_{alu,xu}.sum and smsp__inst_executed.sum over one
 # C2 launch divided by its 40 * 2^24 / 32 warp-steps):
-GRAY_MIX = {"alu": 260, "xu": 72, "issue": 470}
+GRAY_MIX = {"alu": 287.3, "xu": 74.1, "issue": 470.9}
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
 # same capture: the rows are read once into shared memory.
-GRAY_TRAFFIC = None
+GRAY_TRAFFIC = 43520
 
 
 def gray_pipe_bound(sm_count, mhz, mix=None, words=64):
