@@ -97,7 +97,45 @@ def build(verbose: bool = False, force: bool = False, ptxas_info: bool = False) 
     return LIB
 
 
+BINDING_SRC = os.path.join(HERE, "bindings", "_bmmpy.cpp")
+
+
+def binding_path() -> str:
+    import sysconfig
+
+    return os.path.join(HERE, "_bmmpy" + (sysconfig.get_config_var("EXT_SUFFIX") or ".so"))
+
+
+def build_binding(verbose: bool = False, force: bool = False) -> str:
+    """The pybind11 module bmmpy_b200/_bmmpy*.so (the reference's native module
+    name) over include/bmmpy/, linked to libbmm_b200.so next to it."""
+    import sysconfig
+
+    import pybind11
+
+    out = binding_path()
+    deps = [BINDING_SRC, LIB] + sorted(glob.glob(os.path.join(ROOT, "include", "bmmpy", "**",
+                                                              "*.hpp"), recursive=True))
+    if not force and os.path.exists(out) and all(os.path.getmtime(p) <= os.path.getmtime(out)
+                                                  for p in deps):
+        return out
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-shared", "-fPIC", "-fvisibility=hidden",
+           "-I", pybind11.get_include(), "-I", sysconfig.get_paths()["include"],
+           "-I", os.path.join(ROOT, "include"), BINDING_SRC, "-o", out + ".tmp",
+           "-L", HERE, "-lbmm_b200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        sys.stderr.write(proc.stdout + proc.stderr)
+        raise RuntimeError("g++ failed building the _bmmpy module")
+    os.replace(out + ".tmp", out)
+    return out
+
+
 if __name__ == "__main__":
     build(verbose="--verbose" in sys.argv, force="--force" in sys.argv,
           ptxas_info="--ptxas" in sys.argv)
+    build_binding(verbose="--verbose" in sys.argv, force="--force" in sys.argv)
     print(LIB)
