@@ -152,6 +152,9 @@ SIGNATURES = {
     "bmm_gray_tune": [C.c_int, C.c_int],
     "bmm_gray_tune_lanes": [C.c_int],
     "bmm_spectrum_tune": [C.c_int],
+    "bmm_gray_tune_shape": [_sz, _sz, C.c_int, C.c_int, C.c_int],
+    "bmm_spectrum_tune_shape": [_sz, C.c_int],
+    "bmm_tune_reset": [],
     "bmm_spectrum_low_bits": [_sz],
     "bmm_spectrum_topk_slices_dev": [_vp, _sz, _sz, _sz, _sz, C.c_int, C.c_int64, C.c_int64, _vp,
                                      _vp],

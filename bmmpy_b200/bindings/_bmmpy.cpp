@@ -112,6 +112,12 @@ PYBIND11_MODULE(_bmmpy, m) {
              [](const Candidate& c, std::size_t r) {
                  return r / 64 < c.mask.size() && ((c.mask[r / 64] >> (r % 64)) & 1u);
              })
+        .def("__contains__",
+             [](const Candidate& c, std::size_t r) {
+                 return r / 64 < c.mask.size() && ((c.mask[r / 64] >> (r % 64)) & 1u);
+             })
+        .def("__iter__",
+             [](const Candidate& c) { return py::iter(py::cast(c.selected_rows())); })
         .def("__repr__",
              [](const Candidate& c) {
                  std::ostringstream s;

@@ -52,6 +52,9 @@ class Candidate:
                 w &= w - 1
         return out
 
+    def __iter__(self):
+        return iter(self.selected_rows())
+
     @property
     def rows(self) -> list[int]:
         return self.selected_rows()

@@ -292,6 +292,45 @@ int bmm_gray_tune_lanes(int lanes) {
     return BMM_OK;
 }
 
+int bmm_gray_tune_shape(size_t words_per_row, size_t k, int hs_blocks, int chunk_bits,
+                        int lanes) {
+    clear_error();
+    if (words_per_row == 0 || k == 0 || k > 40)
+        return fail(BMM_EINVAL, "gray tuning: words_per_row must be > 0 and k in [1, 40]");
+    if (hs_blocks < -1 || hs_blocks > 8 || hs_blocks == 1 || hs_blocks == 7)
+        return fail(BMM_EINVAL, "gray tuning: hs_blocks must be -1, 0, 2-6 or 8");
+    if (chunk_bits < -1 || chunk_bits > 31)
+        return fail(BMM_EINVAL, "gray tuning: chunk_bits must be -1 or in [0, 31]");
+    if (lanes != -1 && lanes != 1 && lanes != 2)
+        return fail(BMM_EINVAL, "gray tuning: lanes must be -1, 1 or 2");
+    if (lanes == 2 && hs_blocks > 4)
+        return fail(BMM_EINVAL, "gray tuning: 32-word lanes take at most 4 carry-save blocks");
+    GrayTuning t;
+    t.hs_blocks = hs_blocks;
+    t.chunk_bits = chunk_bits;
+    t.lanes = lanes;
+    return gray_tune_shape(words_per_row, (int)k, t);
+}
+
+int bmm_spectrum_tune_shape(size_t t, int low_bits) {
+    clear_error();
+    if (t < 15 || t > 40)
+        return fail(BMM_EINVAL, "spectrum tuning: t must be in [15, 40]");
+    if (low_bits != -1 && (low_bits < 14 || low_bits > (int)(t < 33 ? t : 33)))
+        return fail(BMM_EINVAL, "spectrum tuning: low_bits must be -1 or in [14, min(t, 33)]");
+    g_spectrum_shape_low_bits[t] = low_bits;
+    return BMM_OK;
+}
+
+int bmm_tune_reset(void) {
+    clear_error();
+    gray_tune_reset();
+    for (int& v : g_spectrum_shape_low_bits)
+        v = -1;
+    g_spectrum_low_bits = -1;
+    return BMM_OK;
+}
+
 int bmm_probe_xor_popc(double* words_per_second) {
     clear_error();
     if (!words_per_second)
@@ -512,8 +551,9 @@ static int gray_targets_common(Workspace* ws, const uint64_t* d_words, size_t ro
         lanes = (int)G;
     }
     int chunk = targets_chunk_bits((int)k, lanes, ws->sm_count, (int)n_targets);
-    if (g_gray_tuning.chunk_bits > 0)
-        chunk = g_gray_tuning.chunk_bits;
+    const GrayTuning tune = gray_tuning_for(W, (int)k);
+    if (tune.chunk_bits > 0)
+        chunk = tune.chunk_bits;
     if (chunk > (int)k)
         chunk = (int)k;
     void* d_keys = nullptr;

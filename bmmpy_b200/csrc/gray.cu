@@ -21,6 +21,7 @@
 #include "topk.cuh"
 
 #include <mutex>
+#include <vector>
 
 namespace bmm {
 namespace {
@@ -289,9 +290,9 @@ int group_shape(size_t W, int* wpl, int* g) {
 // The per-target kernel may split a 33-64-word row over a lane pair (32 words
 // each): half the registers per lane, so more warps fit per SM, for one
 // shuffle-add per step.
-int targets_shape(size_t W, int* wpl, int* g) {
+int targets_shape(size_t W, int lanes, int* wpl, int* g) {
     BMM_TRY(group_shape(W, wpl, g));
-    if (*wpl == 64 && *g == 1 && W > 32 && g_gray_tuning.lanes == 2)
+    if (*wpl == 64 && *g == 1 && W > 32 && lanes == 2)
         *wpl = 32, *g = 2;
     return BMM_OK;
 }
@@ -331,6 +332,52 @@ int dispatch_e(int kk, F&& f) {
 }  // namespace
 
 GrayTuning g_gray_tuning;
+
+namespace {
+struct GrayShapeEntry {
+    size_t W;
+    int k;
+    GrayTuning t;
+};
+std::mutex g_shape_mu;
+std::vector<GrayShapeEntry> g_shapes;
+}  // namespace
+
+int gray_tune_shape(size_t W, int k, const GrayTuning& t) {
+    std::lock_guard<std::mutex> lock(g_shape_mu);
+    for (auto& e : g_shapes)
+        if (e.W == W && e.k == k) {
+            e.t = t;
+            return BMM_OK;
+        }
+    if (g_shapes.size() >= 4096)
+        return fail(BMM_EINVAL, "gray tuning: at most 4096 shapes");
+    g_shapes.push_back({W, k, t});
+    return BMM_OK;
+}
+
+void gray_tune_reset() {
+    std::lock_guard<std::mutex> lock(g_shape_mu);
+    g_shapes.clear();
+    g_gray_tuning = GrayTuning{};
+}
+
+GrayTuning gray_tuning_for(size_t W, int k) {
+    GrayTuning t;
+    {
+        std::lock_guard<std::mutex> lock(g_shape_mu);
+        for (const auto& e : g_shapes)
+            if (e.W == W && e.k == k)
+                t = e.t;
+    }
+    if (g_gray_tuning.hs_blocks != -1)
+        t.hs_blocks = g_gray_tuning.hs_blocks;
+    if (g_gray_tuning.chunk_bits != -1)
+        t.chunk_bits = g_gray_tuning.chunk_bits;
+    if (g_gray_tuning.lanes != -1)
+        t.lanes = g_gray_tuning.lanes;
+    return t;
+}
 
 int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items) {
     // Enough independent prefixes for ~32 waves of 128-thread CTAs at 3 CTAs
@@ -414,7 +461,8 @@ int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int 
                         int tiebreak, int chunk, unsigned long long* d_keys, uint64_t* d_best_mask,
                         uint32_t* d_best_weight, cudaStream_t stream) {
     int wpl = 0, g = 0;
-    BMM_TRY(targets_shape((size_t)W, &wpl, &g));
+    const GrayTuning tune = gray_tuning_for((size_t)W, k);
+    BMM_TRY(targets_shape((size_t)W, tune.lanes, &wpl, &g));
     const size_t smem = (size_t)(k + 1) * row_stride(wpl, g) * 8;
     if (smem > (size_t)ws->smem_optin)
         return fail(BMM_EINVAL, "gray targets: %zu bytes of rows exceed shared memory", smem);
@@ -449,7 +497,7 @@ int gray_targets_launch(Workspace* ws, const uint64_t* d_words, int stride, int 
             return tiebreak ? go(gray_targets_kernel<WPL, G, NHB, 1>)
                             : go(gray_targets_kernel<WPL, G, NHB, 0>);
         };
-        const int hs = g_gray_tuning.hs_blocks;
+        const int hs = tune.hs_blocks;
         if constexpr (WPL == 64 && G == 1) {
             switch (hs) {
             case -1: break;
@@ -634,8 +682,9 @@ extern "C" BMM_API int bmm_gray_targets_noalloc(const uint64_t* d_words, size_t 
     while ((size_t)lanes * 64 < W)
         lanes *= 2;
     int chunk = targets_chunk_bits((int)k, lanes, d->sm_count, (int)n_targets);
-    if (g_gray_tuning.chunk_bits > 0)  // the same tuning bmm_gray_targets_dev honours
-        chunk = g_gray_tuning.chunk_bits;
+    const GrayTuning tune = gray_tuning_for(W, (int)k);  // as bmm_gray_targets_dev
+    if (tune.chunk_bits > 0)
+        chunk = tune.chunk_bits;
     if (chunk > (int)k)
         chunk = (int)k;
     // gray_targets_launch clears the keys it uses to ~0 before the search, so

@@ -14,6 +14,14 @@ struct GrayTuning {
 };
 extern GrayTuning g_gray_tuning;
 
+// Per-shape settings found by the autotuner for rows of W words searched
+// against k others (bmm_gray_tune_shape); -1 fields keep the built-in policy.
+int gray_tune_shape(size_t W, int k, const GrayTuning& t);
+void gray_tune_reset();
+// The effective tuning for a shape: the shape entry, overridden field by
+// field by the process-wide g_gray_tuning where that is set.
+GrayTuning gray_tuning_for(size_t W, int k);
+
 // Low chunk width giving enough independent prefixes to fill the device.
 int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items);
 // The same for the per-target kernel (its occupancy and walk length).

@@ -541,13 +541,18 @@ int grid_for(Workspace* ws, long long ntiles) {
 }  // namespace
 
 int g_spectrum_low_bits = -1;
+int g_spectrum_shape_low_bits[41] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
+                                     -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
+                                     -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
 
 int spectrum_low_bits(int t) {
     const int top = t < 33 ? t : 33;
-    if (g_spectrum_low_bits > 0 && t > kTileLog)
-        return g_spectrum_low_bits < kTileLog ? kTileLog
-                                              : (g_spectrum_low_bits > top ? top : g_spectrum_low_bits);
-    return top;
+    if (t <= kTileLog || t > 40)
+        return top;
+    int want = g_spectrum_low_bits > 0 ? g_spectrum_low_bits : g_spectrum_shape_low_bits[t];
+    if (want <= 0)
+        return top;
+    return want < kTileLog ? kTileLog : (want > top ? top : want);
 }
 
 int spectrum_topk_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, long long cols,

@@ -26,6 +26,8 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
 // set (bmm_spectrum_tune), else min(t, 33).
 int spectrum_low_bits(int t);
 extern int g_spectrum_low_bits;
+// Per-t low bits found by the autotuner (bmm_spectrum_tune_shape); -1 = none.
+extern int g_spectrum_shape_low_bits[41];
 
 // In-place transform of 2^t int32 in device memory, t >= 14.
 int spectrum_dense_fwht(Workspace* ws, int32_t* d, int t, cudaStream_t stream);

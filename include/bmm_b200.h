@@ -118,6 +118,19 @@ BMM_API int bmm_gray_tune(int hs_blocks, int chunk_bits);
  * 1 (a lane holds the whole row) or 2 (a lane pair, 32 words each, more
  * warps per SM); -1 = built-in policy.  Results never change, only speed. */
 BMM_API int bmm_gray_tune_lanes(int lanes);
+/* Per-shape autotuner entries (no reference counterpart): for per-target
+ * Gray searches of rows of words_per_row words against k others, use
+ * hs_blocks / chunk_bits / lanes (each -1 = built-in policy; same ranges as
+ * above, at most 4 blocks with lanes = 2).  The process-wide settings of
+ * bmm_gray_tune / bmm_gray_tune_lanes, where set, take precedence.
+ * bmm_spectrum_tune_shape records the spectrum split (low_bits, see
+ * bmm_spectrum_topk_slices_dev) for t-row windows, 15 <= t <= 40; a
+ * bmm_spectrum_tune setting takes precedence.  bmm_tune_reset drops every
+ * entry and setting.  Results never change, only speed. */
+BMM_API int bmm_gray_tune_shape(size_t words_per_row, size_t k, int hs_blocks, int chunk_bits,
+                                int lanes);
+BMM_API int bmm_spectrum_tune_shape(size_t t, int low_bits);
+BMM_API int bmm_tune_reset(void);
 
 /* ---- batched per-target searches (thousands of uneven instances) ----
  * Instance i is a rows x cols matrix stored at words + word_offset with

@@ -74,8 +74,15 @@ def test_native_matrix_and_errors(nb):
         nb.CudaMitmFwhtSearch().search(big.row_window(list(range(16))))
     with pytest.raises(ValueError):
         nb.fwht_inplace(np.zeros(3, np.int32))
-    c = nb.Candidate.from_u64(0b1011, 7)
-    assert (len(c), c.rows, c.has_row(3), c.has_row(2)) == (3, [0, 1, 3], True, False)
+    for c in (nb.Candidate.from_u64(0b1011, 7), bmm_candidate(0b1011, 7)):
+        assert (len(c), c.rows, c.has_row(3), c.has_row(2)) == (3, [0, 1, 3], True, False)
+        assert list(c) == [0, 1, 3] and 3 in c and 2 not in c
+
+
+def bmm_candidate(mask, weight):
+    import bmmpy
+
+    return bmmpy.Candidate.from_u64(mask, weight)
 
 
 @pytest.mark.gpu
