@@ -675,6 +675,14 @@ int bmm_spectrum_tune(int low_bits) {
     return BMM_OK;
 }
 
+int bmm_spectrum_tune_last_pass(int double_buffered) {
+    clear_error();
+    if (double_buffered != 0 && double_buffered != 1)
+        return fail(BMM_EINVAL, "spectrum tuning: double_buffered must be 0 or 1");
+    g_spectrum_last_db = double_buffered;
+    return BMM_OK;
+}
+
 int bmm_spectrum_low_bits(size_t t) { return t > 40 ? -1 : spectrum_low_bits((int)t); }
 
 int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols, size_t k,

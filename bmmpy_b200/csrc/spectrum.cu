@@ -329,8 +329,8 @@ __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
 // holds a loaded value or its address.  The last pass (one CTA per SM, its
 // scan is the longer phase) double-buffers: tile n+1 is in flight while
 // tile n is transformed and scanned.
-template <int R, bool LAST, int E>
-__global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
+template <int R, bool LAST, int E, bool DB = true>
+__global__ void __launch_bounds__(kThr, (LAST && DB) ? 1 : 2)
     pass_mid_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
                     const unsigned long long* __restrict__ total, int kk,
                     bmm_candidate* __restrict__ cta_out) {
@@ -366,11 +366,11 @@ __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
         asm volatile("cp.async.commit_group;" ::: "memory");
     };
     long long tile = blockIdx.x;
-    if (LAST && tile < ntiles)
+    if (LAST && DB && tile < ntiles)
         issue(tile, s);
     for (int it = 0; tile < ntiles; ++it, tile += gridDim.x) {
-        int32_t* cur = LAST ? s + (it & 1) * kTile : s;
-        if (LAST) {
+        int32_t* cur = (LAST && DB) ? s + (it & 1) * kTile : s;
+        if (LAST && DB) {
             const long long nxt = tile + gridDim.x;
             if (nxt < ntiles) {
                 issue(nxt, s + ((it + 1) & 1) * kTile);
@@ -488,10 +488,12 @@ constexpr size_t pass_smem(bool last, int E) {
                : kTile * sizeof(int32_t);
 }
 
-// The last middle pass double-buffers its tiles.
-constexpr size_t mid_smem(bool last, int E) {
-    return last ? (pass_smem(true, E) > 2 * kTile * sizeof(int32_t) ? pass_smem(true, E)
-                                                                   : 2 * kTile * sizeof(int32_t))
+// The last middle pass double-buffers its tiles (one CTA per SM), or runs two
+// single-buffered CTAs per SM within 128 registers (g_spectrum_last_db = 0).
+constexpr size_t mid_smem(bool last, int E, bool db = true) {
+    return last ? (pass_smem(true, E) > (db ? 2 : 1) * kTile * sizeof(int32_t)
+                       ? pass_smem(true, E)
+                       : (db ? 2 : 1) * kTile * sizeof(int32_t))
                 : kTile * sizeof(int32_t);
 }
 
@@ -499,10 +501,13 @@ template <int E>
 int launch_mid(int R, bool last, int32_t* d, int T, int lo, unsigned long long xhi,
                const unsigned long long* total, int kk, bmm_candidate* lists, int grid,
                cudaStream_t st) {
-    const size_t smem = mid_smem(last, E);
+    const bool db = g_spectrum_last_db != 0;
+    const size_t smem = mid_smem(last, E, db);
 #define BMM_MID(RR)                                                                               \
     case RR: {                                                                                    \
-        auto k = last ? pass_mid_kernel<RR, true, E> : pass_mid_kernel<RR, false, E>;             \
+        auto k = last ? (db ? pass_mid_kernel<RR, true, E, true>                                  \
+                            : pass_mid_kernel<RR, true, E, false>)                                \
+                      : pass_mid_kernel<RR, false, E>;                                            \
         BMM_CUDA_TRY(                                                                             \
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
         k<<<grid, kThr, smem, st>>>(d, T, lo, xhi, total, kk, lists);                             \
@@ -541,6 +546,7 @@ int grid_for(Workspace* ws, long long ntiles) {
 }  // namespace
 
 int g_spectrum_low_bits = -1;
+int g_spectrum_last_db = 1;
 int g_spectrum_shape_low_bits[41] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
                                      -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
                                      -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
@@ -628,7 +634,9 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
     const int grid_m = grid_for(ws, ntiles);  // every pass has 2^(T-14) tiles
     // the double-buffered last middle pass: one persistent CTA per SM
     const int grid_last =
-        nmid ? (int)std::min<long long>(ntiles, (long long)ws->sm_count) : grid_a;
+        nmid ? (int)std::min<long long>(ntiles, (long long)ws->sm_count *
+                                                    (g_spectrum_last_db != 0 ? 1 : 2))
+             : grid_a;
     const long long slices = slice_end - slice_begin;
     bmm_candidate *lists = nullptr, *slice_lists = nullptr;
     BMM_TRY(ws_buffer(ws, kSlotCand, (size_t)grid_last * kk * sizeof(bmm_candidate),

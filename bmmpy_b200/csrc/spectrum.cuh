@@ -26,6 +26,9 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
 // set (bmm_spectrum_tune), else min(t, 33).
 int spectrum_low_bits(int t);
 extern int g_spectrum_low_bits;
+// Last transform pass: 1 = one double-buffered CTA per SM, 0 = two
+// single-buffered CTAs per SM.
+extern int g_spectrum_last_db;
 // Per-t low bits found by the autotuner (bmm_spectrum_tune_shape); -1 = none.
 extern int g_spectrum_shape_low_bits[41];
 

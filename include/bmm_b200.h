@@ -585,6 +585,10 @@ BMM_API int bmm_search_apply_dev(uint64_t* words, size_t rows, size_t stride, si
  * bmm_spectrum_tune sets the default split (-1: min(t, 33)); results never
  * change, only speed and memory (2^low_bits int32 per call). */
 BMM_API int bmm_spectrum_tune(int low_bits);
+/* The spectrum's last transform pass (fused with the top-k scan): 1 = one
+ * double-buffered CTA per SM (default), 0 = two single-buffered CTAs per SM.
+ * Results never change, only speed. */
+BMM_API int bmm_spectrum_tune_last_pass(int double_buffered);
 BMM_API int bmm_spectrum_low_bits(size_t t);
 BMM_API int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols,
                                          size_t k, int low_bits, int64_t slice_begin,
