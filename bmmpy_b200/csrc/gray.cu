@@ -20,6 +20,7 @@
 #include "popc.cuh"
 #include "topk.cuh"
 
+#include <cmath>
 #include <mutex>
 #include <vector>
 
@@ -400,22 +401,26 @@ int auto_chunk_bits(int t, int lanes_per_prefix, int sm_count, int n_items) {
 }
 
 int targets_chunk_bits(int k, int lanes_per_prefix, int sm_count, int n_targets) {
-    // The per-target kernel runs 2 CTAs per SM (234 registers: the schedule
-    // the compiler picks at that budget beat 3 CTAs per SM by 8 %); aim for
-    // enough prefixes to fill ~16 waves, but walk at least 2^10 Gray steps per
-    // prefix so the prefix set-up (up to k - chunk row XORs) stays near 1 %.
-    // Measured on 40 x 4096, k = 24: chunk 10 takes 13.49 ms, chunk 8 13.60.
-    const double want =
-        (double)sm_count * 2 * 16 * kThreads / lanes_per_prefix / (n_targets ? n_targets : 1);
-    int hb = 0;
-    while (hb < k && (double)(1ull << hb) < want)
-        ++hb;
-    int chunk = k - hb;
-    if (chunk < 10)
-        chunk = k < 10 ? k : 10;
-    if (chunk > 20)
-        chunk = 20;
-    return chunk > k ? k : chunk;
+    // Waves of 128-thread CTAs the launch fills at 2 CTAs per SM (the
+    // kernel's 234-register schedule) when each prefix walks 2^chunk states.
+    auto waves = [&](int chunk) {
+        return std::ldexp((double)(n_targets > 0 ? n_targets : 1) * lanes_per_prefix, k - chunk) /
+               ((double)sm_count * 2 * kThreads);
+    };
+    // Long walks keep the prefix set-up (up to k - chunk row XORs) near 1 %;
+    // many waves keep the last wave's tail small.  Large jobs: the longest
+    // walk (>= 2^10) that still fills 16 waves; small jobs: the longest walk
+    // (>= 2^8) that fills 4 waves, else 2^8.  Measured optima on B200: 40 x
+    // 4096, k = 24 -> 10 (13.49 ms); 40 x 2048, k = 20 -> 8 (0.52 ms vs 0.84
+    // at 10); 64 x 256, k = 16 -> 8 (0.035 ms vs 0.112 at 10).
+    const int top = k < 20 ? k : 20;
+    for (int c = top; c >= 10; --c)
+        if (waves(c) >= 16)
+            return c;
+    for (int c = top; c >= 8; --c)
+        if (waves(c) >= 4)
+            return c;
+    return k < 8 ? k : 8;
 }
 
 int gray_window_launch(Workspace* ws, const uint64_t* d_rows, int t, int W, int chunk, int kk,
