@@ -445,8 +445,38 @@ def run_ga(args):
         entry["learned_vs_uniform"] = {"threshold_uniform_best": ulr, "uniform_s": tu,
                                        "learned_s": tl}
         seeds_out.append(entry)
+    def spread(vals):
+        vals = sorted(v for v in vals if v is not None)
+        if not vals:
+            return None
+        q = lambda f: float(np.quantile(vals, f))  # noqa: E731
+        return {"median": q(0.5), "q25": q(0.25), "q75": q(0.75), "min": vals[0],
+                "max": vals[-1], "n": len(vals)}
+
+    def ratio(a, b):
+        return a / b if a is not None and b else None
+
     speedups = [e["off"]["time_to_threshold_s"] / e["learned"]["time_to_threshold_s"]
                 for e in seeds_out if e["learned"]["time_to_threshold_s"]]
+    summary = {
+        "learned_vs_plain": spread(ratio(e["off"]["time_to_threshold_s"],
+                                         e["learned"]["time_to_threshold_s"]) for e in seeds_out),
+        "uniform_vs_plain": spread(ratio(e["off"]["time_to_threshold_s"],
+                                         e["uniform"]["time_to_threshold_s"]) for e in seeds_out),
+        "learned_vs_uniform": spread(ratio(e["learned_vs_uniform"]["uniform_s"],
+                                           e["learned_vs_uniform"]["learned_s"])
+                                     for e in seeds_out),
+        "paired_rate_learned": spread(e["learned"]["proposal"]["paired_rate_learned"]
+                                      for e in seeds_out if e["learned"].get("proposal")),
+        "paired_rate_uniform_in_learned_runs": spread(
+            e["learned"]["proposal"]["paired_rate_uniform"]
+            for e in seeds_out if e["learned"].get("proposal")),
+        "reached_planted": {m: sum(e[m]["reached_planted"] for e in seeds_out)
+                            for m in ("off", "uniform", "learned")},
+        "note": "ratios are time-to-threshold quotients (>1: the first variant is faster); "
+                "learned_vs_uniform uses the uniform-window run's best at the cap as the "
+                "threshold",
+    }
     line = {
         "metric": "time-to-threshold speed-up, learned vs plain GA (threshold: the plain GA's "
                   "best weight within the cap)",
@@ -458,6 +488,7 @@ def run_ga(args):
                    "population": args.population, "migration": "ring, every 20 generations",
                    "cap_s": args.cap, "planted_weight": planted,
                    "proposal": "32 queries per elite, 16-row windows, 1 Adam step/generation"},
+        "summary": summary,
         "seeds": seeds_out,
     }
     print(json.dumps(line), flush=True)

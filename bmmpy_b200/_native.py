@@ -82,7 +82,8 @@ class GaProposalStats_t(C.Structure):
     _fields_ = [("tried_learned", C.c_uint64), ("improved_learned", C.c_uint64),
                 ("tried_uniform", C.c_uint64), ("improved_uniform", C.c_uint64),
                 ("examples", C.c_uint64), ("last_loss", C.c_float),
-                ("learned_fraction", C.c_float)]
+                ("learned_fraction", C.c_float), ("paired_generations", C.c_uint64),
+                ("paired_rate_learned", C.c_double), ("paired_rate_uniform", C.c_double)]
 
 
 class GaMigration_t(C.Structure):

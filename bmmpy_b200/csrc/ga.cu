@@ -1960,6 +1960,9 @@ BMM_API int bmm_ga_get_proposal_stats(bmm_ga* g, bmm_ga_proposal_stats* out) {
     out->examples = g->examples;
     out->last_loss = g->last_loss;
     out->learned_fraction = g->prop.learned_frac;
+    out->paired_generations = g->paired_gens;
+    out->paired_rate_learned = g->paired_gens ? g->paired_rate[0] / (double)g->paired_gens : 0.0;
+    out->paired_rate_uniform = g->paired_gens ? g->paired_rate[1] / (double)g->paired_gens : 0.0;
     return BMM_OK;
 }
 

@@ -143,6 +143,8 @@ struct bmm_ga {
     unsigned long long examples = 0;
     float last_loss = 0.f;
     double ema_tried[2] = {0, 0}, ema_improved[2] = {0, 0};  // learned, uniform (decayed)
+    double paired_rate[2] = {0, 0};  // per-generation rates summed over paired generations
+    unsigned long long paired_gens = 0;
     int replay_head = 0, replay_fill = 0;
 };
 

@@ -452,6 +452,11 @@ int propose_generation(bmm_ga* g) {
         // learned share: decayed success counts of both window sources;
         // the learned share moves towards the better one
         const unsigned long long* k = g->h_counters;
+        if (k[0] > 0 && k[2] > 0) {
+            g->paired_rate[0] += (double)k[1] / (double)k[0];
+            g->paired_rate[1] += (double)k[3] / (double)k[2];
+            ++g->paired_gens;
+        }
         for (int src = 0; src < 2; ++src) {
             g->ema_tried[src] = 0.95 * g->ema_tried[src] + (double)k[2 * src];
             g->ema_improved[src] = 0.95 * g->ema_improved[src] + (double)k[2 * src + 1];

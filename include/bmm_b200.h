@@ -355,6 +355,13 @@ typedef struct bmm_ga_proposal_stats {
     uint64_t examples;      /* training examples used */
     float last_loss;        /* cross-entropy of the last training step */
     float learned_fraction; /* current share of learned windows */
+    /* Improvement rates of learned and uniform windows averaged over the
+     * generations that drew both (each generation weighs the same): a fair
+     * comparison, whereas the totals above mix early generations, where
+     * every window improves often, with late ones in different shares. */
+    uint64_t paired_generations;
+    double paired_rate_learned;
+    double paired_rate_uniform;
 } bmm_ga_proposal_stats;
 BMM_API int bmm_ga_set_proposal(bmm_ga* g, const bmm_ga_proposal* p);
 BMM_API int bmm_ga_get_proposal_stats(bmm_ga* g, bmm_ga_proposal_stats* out);
