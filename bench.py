@@ -44,6 +44,11 @@ the planted 512 x 65536 matrix: ``value`` from the device synergy table,
 payload parsed on the device, BitMatrix.from_text and a binary file loaded
 into device memory end to end.
 
+``--workload c1`` / ``--workload batch`` (1 GPU) measure the per-target
+transform on the 64 x 256 matrix (16 others per target) and on the 4096 uneven
+planted instances in one persistent launch, checked against the reference's
+answers, with an ALU-pipe roofline.
+
 ``--workload mlp`` (1 GPU) measures the proposal network's tcgen05 GEMMs
 (forward and training step on 16384 resident rows).
 
@@ -999,6 +1004,141 @@ def run_io(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# Per-target transform workloads: C1 (64 x 256, 16 others per target) and C4
+# (4096 uneven planted instances in one persistent launch).  The transform of
+# a k = 16 item packs two 16-bit spectrum lanes in one int32 word, so one
+# IADD or ISUB performs two butterflies' halves: one butterfly per ALU op.
+# Bound: the ALU pipe, 64 int32 ops per clock per SM (the FMA pipe takes no
+# part in these adds), i.e. sm_count * 64 * f_SM butterflies/s.
+
+
+def _butterflies(k):
+    return k * (1 << (k - 1)) if k > 0 else 0
+
+
+def run_transform_targets(args):
+    import torch
+
+    from bmmpy_b200 import batch as B
+    from bmmpy_b200 import targets as T
+    from bmmpy_b200.workloads import C1, C4, batch_instance, gen_instance
+    from tests.golden.fixtures import checksum_pairs
+
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "unavailable": "the C1/C4 per-target transform "
+                          "workloads have no reference entry point beyond FwhtSearch per window "
+                          "(bench.py --workload gray --impl reference times the reference "
+                          "searcher)"}))
+        return 0
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream(dev)
+    gold = np.load(os.path.join(ROOT, "tests", "golden", "workloads.npz"))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    if args.workload == "c1":
+        m, _ = gen_instance(C1["rows"], C1["cols"], C1["p"], C1["seed"])
+        t_idx, o_idx = T.cyclic_others(C1["rows"], C1["k"])
+        d_words = torch.from_numpy(m.words.view(np.int64).copy()).to(dev)
+        d_t = torch.from_numpy(t_idx.view(np.int32).copy()).to(dev)
+        d_o = torch.from_numpy(o_idx.view(np.int32).copy()).to(dev)
+        d_m = torch.empty(C1["rows"], dtype=torch.int64, device=dev)
+        d_w = torch.empty(C1["rows"], dtype=torch.int32, device=dev)
+        items, ks = C1["rows"], [C1["k"]] * C1["rows"]
+
+        def launch():
+            T.fwht_targets_dev(d_words, C1["rows"], m.stride_words, C1["cols"], d_t, d_o, C1["k"],
+                               d_m, d_w, stream.cuda_stream)
+
+        def check():
+            assert np.array_equal(d_m.cpu().numpy().view(np.uint64), gold["c1_mask"])
+            assert np.array_equal(d_w.cpu().numpy().view(np.uint32), gold["c1_weight"])
+
+        def e2e():
+            return T.fwht_targets(m, t_idx, o_idx)
+
+        h2d, d2h = m.words.nbytes + t_idx.nbytes + o_idx.nbytes, C1["rows"] * 12
+        workload = ("C1 per-target transform: 64 x 256 Bernoulli(0.5) (seed 0), each row vs "
+                    "all 2^16 XORs of the next 16 rows")
+    else:
+        insts = [batch_instance(i) for i in range(C4["count"])]
+        b = B.Batch([(mm, k) for mm, k, _ in insts])
+        ks = [k for mm, k, _ in insts for _ in range(mm.rows)]
+        items = b.n_out
+        dw = torch.from_numpy(b.words.view(np.int64).copy()).to(dev)
+        d_m = torch.empty(b.n_out, dtype=torch.int64, device=dev)
+        d_w = torch.empty(b.n_out, dtype=torch.int32, device=dev)
+
+        def launch():
+            b.run_dev(dw, d_m, d_w, stream.cuda_stream)
+
+        def check():
+            ms = b.split(d_m.cpu().numpy().view(np.uint64))
+            ws = b.split(d_w.cpu().numpy().view(np.uint32))
+            bad = [i for i, (a, c) in enumerate(zip(ms, ws))
+                   if checksum_pairs(a, c) != int(gold["c4_checksums"][i])]
+            assert not bad, f"{len(bad)} instances differ from the reference"
+
+        def e2e():
+            return b.run()
+
+        h2d, d2h = b.words.nbytes + b.desc.nbytes, b.n_out * 12
+        workload = ("C4 batch: 4096 planted instances, n in [16,128], m in [64,2048] "
+                    "log-uniform, density 0.05, 4n scrambles, k = min(n-1, 16), one "
+                    "persistent launch replayed as a CUDA graph")
+    combos = float(sum(1 << k for k in ks))
+    bfly = float(sum(_butterflies(k) for k in ks))
+    for _ in range(args.warmup):
+        flush.zero_()
+        launch()
+    torch.cuda.synchronize()
+    check()
+    sampler = clock_sampler(None)
+    time.sleep(0.3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    for i in range(args.steps):
+        flush.zero_()
+        evs[i][0].record(stream)
+        launch()
+        evs[i][1].record(stream)
+    torch.cuda.synchronize()
+    time.sleep(0.3)
+    clocks = clock_summary(sampler)
+    ms = sum(a.elapsed_time(c) for a, c in evs) / args.steps
+    check()
+    e_steps = max(3, args.steps // 2)
+    e2e()
+    t0 = time.perf_counter()
+    for _ in range(e_steps):
+        e2e()
+    e_dt = (time.perf_counter() - t0) / e_steps
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = (clocks or {}).get("sm_mhz") or 1965.0
+    peak = sms * 64 * mhz * 1e6
+    achieved = bfly / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": combos / (ms / 1e3), "unit": UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int32 (two int16 lanes packed)",
+        "data": "synthetic (xorshift64 seeded instances)",
+        "config": {"workload": workload, "items": items, "combos_per_step": combos,
+                   "l2": "flushed before every timed step (256 MB device write)"},
+        "e2e": {"value": combos / e_dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": args.steps,
+        "roofline": {"bound": "alu", "achieved": achieved / 1e12, "peak": peak / 1e12,
+                     "unit": "T butterflies/s", "frac": achieved / peak,
+                     "peak_source": f"ALU pipe: {sms} SMs x 64 int32 ops/clk x {mhz:.0f} MHz "
+                                    "sampled; one packed IADD/ISUB = one butterfly",
+                     "traffic": None},
+        "clocks": clocks,
+        "results": "equal to the reference's per-target answers (golden)",
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_mlp(args):
     """The proposal network's tcgen05 GEMMs: forward passes and training steps
     (forward, backward, Adam) on 16384 resident query rows, CUDA-event timed
@@ -1074,7 +1214,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference", "reference-gpu"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="gray", choices=["gray", "ga", "mitm", "basis", "sa", "io", "mlp"])
+    ap.add_argument("--workload", default="gray",
+                    choices=["gray", "ga", "mitm", "basis", "sa", "io", "mlp", "c1", "batch"])
     ap.add_argument("--cap", type=float, default=60.0, help="GA: wall-clock cap per run (s)")
     ap.add_argument("--window", type=int, default=0,
                     help="mitm: window rows (default 32; one sweep = rows / window windows)")
@@ -1095,6 +1236,8 @@ def main():
         return run_io(args)
     if args.workload == "mlp":
         return run_mlp(args)
+    if args.workload in ("c1", "batch"):
+        return run_transform_targets(args)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -22,7 +22,7 @@ C1 = dict(rows=64, cols=256, p=0.5, seed=0, k=16)
 # C2: Gray-code brute force, 40x4096, Bernoulli(0.3), seed 1, k=24 others
 C2 = dict(rows=40, cols=4096, p=0.3, seed=1, k=24)
 # C3: MITM on a planted 512x65536 instance (p=0.02, seed 2, 2000 scrambles)
-C3 = dict(rows=512, cols=65536, p=0.02, seed=2, scrambles=2000, window=32, golden_windows=2)
+C3 = dict(rows=512, cols=65536, p=0.02, seed=2, scrambles=2000, window=32, golden_windows=16)
 # C4: 4096 uneven planted instances (seeds 1000..5095)
 C4 = dict(count=4096, seed0=1000, p=0.05)
 # C5: GA on a planted 256x8192 instance (p=0.01, seed 7, 5000 scrambles)

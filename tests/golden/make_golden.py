@@ -184,17 +184,27 @@ def c4(R, P, arrays):
     print("C4 done", time.time() - t0)
 
 
+def _c3_window(j):
+    # one reference MitmFwhtSearch(k=64) on rows 32j..32j+31 (its search is
+    # single-threaded; windows run in parallel worker processes)
+    R, P = ref(), port()
+    m, _ = P.gen_instance(C3["rows"], C3["cols"], C3["p"], C3["seed"], C3["scrambles"])
+    return np.array(R.mitm_search(m, C3["cols"], list(range(32 * j, 32 * j + 32)), 64), np.uint64)
+
+
 def c3(R, P, arrays):
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+
     t0 = time.time()
     m, planted = P.gen_instance(C3["rows"], C3["cols"], C3["p"], C3["seed"], C3["scrambles"])
     arrays["c3_planted"] = np.array([planted], np.uint64)
-    tops = []
-    for j in range(C3["golden_windows"]):
-        res = R.mitm_search(m, C3["cols"], list(range(32 * j, 32 * j + 32)), 64)
-        tops.append(np.array(res, np.uint64))
-        print("  C3 window", j, time.time() - t0)
+    n = C3["golden_windows"]
+    with ProcessPoolExecutor(max_workers=min(n, os.cpu_count() or 1),
+                             mp_context=mp.get_context("spawn")) as pool:
+        tops = list(pool.map(_c3_window, range(n)))
     arrays["c3_top64"] = np.stack(tops, 0)
-    print("C3 done", time.time() - t0)
+    print("C3 done", n, "windows", time.time() - t0)
 
 
 def ga(R, P, arrays):
