@@ -96,15 +96,16 @@ template <int WL, int E, typename MaskOf>
 __device__ __forceinline__ void scan_values(const int32_t (&x)[64], long long N, int kk,
                                             WarpTopK<E>& top, uint32_t& thr, MaskOf mask_of) {
     const int base = round_base<WL>(threadIdx.x);
-    if (N < (1ll << 30)) {  // |x| <= N: 2*weight = N - x fits 32 bits
-        const uint32_t n32 = (uint32_t)N;
-        uint32_t lo2 = 0xffffffffu;
+    if (N < (1ll << 30)) {
+        // Every spectrum value is a sum of N terms +-1, so N - x is even and
+        // in [0, 2N]: the smallest weight of the 64 values is (N - max x) / 2,
+        // one integer max per value.
+        int32_t hi = x[0];
 #pragma unroll
-        for (int e = 0; e < 64; ++e) {
-            const uint32_t w2 = n32 - (uint32_t)x[e];
-            lo2 = (w2 & 1u) ? lo2 : min(lo2, w2);
-        }
-        if (!__any_sync(kFull, lo2 != 0xffffffffu && (lo2 >> 1) <= thr))
+        for (int e = 1; e < 64; ++e)
+            hi = max(hi, x[e]);
+        const uint32_t lo2 = (uint32_t)N - (uint32_t)hi;
+        if (!__any_sync(kFull, (lo2 >> 1) <= thr))
             return;
     } else {
         long long lo2 = (long long)UINT32_MAX * 2 + 2;
