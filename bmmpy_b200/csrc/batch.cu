@@ -30,7 +30,11 @@ constexpr int kGrayWords = 8;                   // GRAY items hold rows of <= 8 
 enum Method : uint32_t { kFwht16 = 0, kFwhtSmall = 1, kGray = 2 };
 
 struct BatchPolicy {
-    int gray_max_words = 4;  // k = 16 items with W <= this use GRAY
+    // k = 16 items with W <= this use GRAY.  0: the packed transform for every
+    // k = 16 item -- on B200 it beats the Gray enumeration at every row width
+    // up to 8 words (C4 batch: 15.1 ms against 21.5 ms with a 4-word
+    // crossover; bmmpy_b200.autotune measures it per device).
+    int gray_max_words = 0;
     int force = -1;          // -1: policy; else every item uses this method where legal
 };
 BatchPolicy g_policy;

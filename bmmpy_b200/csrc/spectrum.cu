@@ -100,10 +100,16 @@ __device__ __forceinline__ void scan_values(const int32_t (&x)[64], long long N,
         // Every spectrum value is a sum of N terms +-1, so N - x is even and
         // in [0, 2N]: the smallest weight of the 64 values is (N - max x) / 2,
         // one integer max per value.
-        int32_t hi = x[0];
+        // eight independent running maxima, then a tree (no 64-long chain)
+        int32_t h8[8];
 #pragma unroll
-        for (int e = 1; e < 64; ++e)
-            hi = max(hi, x[e]);
+        for (int j = 0; j < 8; ++j)
+            h8[j] = x[j];
+#pragma unroll
+        for (int e = 8; e < 64; ++e)
+            h8[e & 7] = max(h8[e & 7], x[e]);
+        const int32_t hi = max(max(max(h8[0], h8[1]), max(h8[2], h8[3])),
+                               max(max(h8[4], h8[5]), max(h8[6], h8[7])));
         const uint32_t lo2 = (uint32_t)N - (uint32_t)hi;
         if (!__any_sync(kFull, (lo2 >> 1) <= thr))
             return;

@@ -168,8 +168,9 @@ BMM_API int bmm_batch_targets(const uint64_t* words, size_t n_words, const bmm_i
                               size_t n_inst, uint64_t* best_mask, uint32_t* best_weight);
 /* Autotuner hook (no reference counterpart): k = 16 items whose rows have at
  * most gray_max_words words (0..8) use the Gray enumeration instead of the
- * transform; force_method (-1 none, 0/1 transform, 2 Gray) overrides where
- * legal.  Applies to plans created afterwards; results never change. */
+ * transform (default 0: the transform everywhere); force_method (-1 none,
+ * 0/1 transform, 2 Gray) overrides where legal.  Applies to plans created
+ * afterwards; results never change. */
 BMM_API int bmm_batch_policy(int gray_max_words, int force_method);
 
 /* Roofline probe for the Gray-code kernels: runs a register-only kernel with
