@@ -12,14 +12,19 @@
 // to six bits over a bank-swizzled tile):
 //   pass A (bits 0..13): each tile is BUILT from the columns whose pattern
 //       falls in it (columns bucketed by tile with a counting sort), so the
-//       sparse histogram is never written; empty tiles are written as zeros;
+//       sparse histogram is never written; empty tiles (all-zero transforms)
+//       are not written at all, and the next pass zero-fills their rows from
+//       the bucket offsets instead of reading them;
 //   middle passes (<= 9 bits, 32 consecutive elements per row so every warp
 //       access is a full 128-byte line): read, transform, write;
 //   the last pass keeps its values in registers and feeds the weight + top-k
 //       scan instead of writing (warp-register top-k lists, merged at the end).
 // For t > 33 the extra high bits are enumerated (meet-in-the-middle): slice x
 // transforms the low 33 bits of the histogram signed by parity(high & x).
-// Traffic for t = 32: write 16 GB + read/write 32 GB + read 16 GB.
+// Traffic for t = 32: write 16 GB x (share of nonempty pass-A tiles) + read
+// the same + write 16 GB + read 16 GB (64 GB when every tile is nonempty).
+// The middle / last passes move tiles with 16-byte cp.async; a source size
+// of 0 zero-fills without a read.
 #include "common.cuh"
 #include "spectrum.cuh"
 #include "topk.cuh"
@@ -280,12 +285,11 @@ __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
         int32_t* gt = d + (size_t)tile * kTile;
         if (SPARSE) {
             const unsigned b0 = offsets[tile], b1 = offsets[tile + 1];
-            if (b0 == b1 && !LAST) {  // empty tile: its transform is zero
-                int4* g4 = reinterpret_cast<int4*>(gt);
-                for (int i = tid; i < kTile / 4; i += kThr)
-                    g4[i] = make_int4(0, 0, 0, 0);
+            // An empty tile's transform is zero and is never written: the
+            // next pass (bits 14.., the only reader) zero-fills its rows from
+            // the same offsets instead of reading them.
+            if (b0 == b1 && !LAST)
                 continue;
-            }
             int4* s4 = reinterpret_cast<int4*>(s);
             for (int i = tid; i < kTile / 4; i += kThr)
                 s4[i] = make_int4(0, 0, 0, 0);
@@ -340,7 +344,8 @@ template <int R, bool LAST, int E, bool DB = true>
 __global__ void __launch_bounds__(kThr, (LAST && DB) ? 1 : 2)
     pass_mid_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
                     const unsigned long long* __restrict__ total, int kk,
-                    bmm_candidate* __restrict__ cta_out) {
+                    bmm_candidate* __restrict__ cta_out,
+                    const unsigned* __restrict__ empty_offsets) {
     static_assert(R >= 1 && R <= 9, "R in [1, 9]");
     constexpr int B = kTileLog - R;
     extern __shared__ __align__(16) int32_t s[];
@@ -365,9 +370,16 @@ __global__ void __launch_bounds__(kThr, (LAST && DB) ? 1 : 2)
         for (int u = 0; u < kTile / 4 / kThr; ++u) {
             const int k = (u * kThr + tid) * 4;
             const uint64_t gi = gb | ((uint64_t)(k >> B) << lo) | (uint64_t)(k & ((1 << B) - 1));
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(
+            // rows of pass-A tiles that were empty (never written) are
+            // zero-filled: 0 source bytes, nothing is read
+            uint32_t src_bytes = 16;
+            if (empty_offsets) {
+                const uint64_t at = gi >> kTileLog;
+                src_bytes = empty_offsets[at] == empty_offsets[at + 1] ? 0u : 16u;
+            }
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
                              sb + 4u * (uint32_t)swzm(k)),
-                         "l"(d + gi)
+                         "l"(d + gi), "r"(src_bytes)
                          : "memory");
         }
         asm volatile("cp.async.commit_group;" ::: "memory");
@@ -507,8 +519,8 @@ constexpr size_t mid_smem(bool last, int E, bool db = true) {
 template <int E>
 int launch_mid(int R, bool last, int32_t* d, int T, int lo, unsigned long long xhi,
                const unsigned long long* total, int kk, bmm_candidate* lists, int grid,
-               cudaStream_t st) {
-    const bool db = g_spectrum_last_db != 0;
+               cudaStream_t st, const unsigned* empty_offsets = nullptr) {
+    const bool db = g_spectrum_last_db != 0 || E > 4;  // E = 32 lists need the registers
     const size_t smem = mid_smem(last, E, db);
 #define BMM_MID(RR)                                                                               \
     case RR: {                                                                                    \
@@ -517,7 +529,7 @@ int launch_mid(int R, bool last, int32_t* d, int T, int lo, unsigned long long x
                       : pass_mid_kernel<RR, false, E>;                                            \
         BMM_CUDA_TRY(                                                                             \
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
-        k<<<grid, kThr, smem, st>>>(d, T, lo, xhi, total, kk, lists);                             \
+        k<<<grid, kThr, smem, st>>>(d, T, lo, xhi, total, kk, lists, empty_offsets);              \
         BMM_CUDA_TRY(cudaGetLastError());                                                         \
         return BMM_OK;                                                                            \
     }
@@ -642,7 +654,7 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
     // the double-buffered last middle pass: one persistent CTA per SM
     const int grid_last =
         nmid ? (int)std::min<long long>(ntiles, (long long)ws->sm_count *
-                                                    (g_spectrum_last_db != 0 ? 1 : 2))
+                                                    (g_spectrum_last_db != 0 || kk > 128 ? 1 : 2))
              : grid_a;
     const long long slices = slice_end - slice_begin;
     bmm_candidate *lists = nullptr, *slice_lists = nullptr;
@@ -680,7 +692,8 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
                 for (int i = 0; i < nmid; ++i) {
                     BMM_TRY(launch_mid<E>(widths[i], i == nmid - 1, (int32_t*)spec, T, lo,
                                           (unsigned long long)x, total, kk, lists,
-                                          i == nmid - 1 ? grid_last : grid_m, stream));
+                                          i == nmid - 1 ? grid_last : grid_m, stream,
+                                          i == 0 ? (const unsigned*)offsets : nullptr));
                     lo += widths[i];
                 }
             }
