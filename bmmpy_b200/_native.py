@@ -205,6 +205,8 @@ SIGNATURES = {
     "bmm_mlp_create_on_stream": [C.c_uint64, C.c_float, _vp, C.POINTER(_vp)],
     "bmm_mlp_forward_dev": [_vp, _vp, _sz, _vp],
     "bmm_mlp_train_dev": [_vp, _vp, _vp, _sz, C.c_int],
+    "bmm_mlp_forward_bf16_dev": [_vp, _vp, _sz, _vp],
+    "bmm_mlp_tune": [C.c_int],
     "bmm_exact_basis": [_u64p, _sz, _sz, _u32p, _sz, C.POINTER(ExactBasisConfig_t),
                         C.POINTER(ExactBasisResult_t), _u32p, _u32p],
     "bmm_basis_weight_counts": [_u64p, _sz, _sz, _u32p, _sz, _u64p],

@@ -411,7 +411,7 @@ int propose_generation(bmm_ga* g) {
         return BMM_OK;
     features_kernel<<<(unsigned)std::min<uint64_t>(Q, 65535), 256, 0, s>>>(st, pb, gen);
     if (pb.mode == 1)
-        BMM_TRY(mlp::forward_dev(g->net, pb.X, 1, (int)Q, pb.logits));
+        BMM_TRY(mlp::forward_dev(g->net, pb.X, 1, (int)Q, pb.logits, false));
     BMM_CUDA_TRY(cudaMemsetAsync(pb.counters, 0, 32, s));
     search_kernel<<<g->search_grid, item::kFwht16Threads, 32768 * 4, s>>>(st, pb, gen,
                                                                           (int)g->cols);

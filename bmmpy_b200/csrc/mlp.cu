@@ -24,6 +24,9 @@
 #include "mlp.cuh"
 #include "umma.cuh"
 
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -226,6 +229,86 @@ __device__ __forceinline__ void stage_any(unsigned char* dst, int rows, int mode
         stage_vec(dst, rows, mode, src, bf16, ld_r, ld_k, row0, nrows, k0, K);
 }
 
+// Epilogue of a 128 x 256 tile: warp w reads TMEM lanes 32 (w % 4).. and
+// columns 128 (w / 4)..; scale, bias, ReLU-backward mask, FP32 / BF16 outputs.
+__device__ __forceinline__ void gemm_epilogue(const GemmArgs& g, uint32_t tmem, int m0, int n0,
+                                              bool empty, float* out_f, const float* s_bias) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int quarter = warp & 3, half = warp >> 2;
+    const int m = m0 + quarter * 32 + lane;
+    for (int c = half * (kBN / 64); c < (half + 1) * (kBN / 64); ++c) {
+        float v[32];
+        umma::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(c * 32), v);
+        if (m >= g.M)
+            continue;
+        if (empty)
+#pragma unroll
+            for (int i = 0; i < 32; ++i)
+                v[i] = 0.f;
+        // 32 consecutive outputs of row m: 16-byte vector loads and stores
+        // where the host found the rows aligned, element by element else
+        const int nb = n0 + c * 32;
+        const bool full = nb + 31 < g.N;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) {
+            float val = v[i] * g.scale;
+            if (s_bias)
+                val += s_bias[c * 32 + i];  // the tile's biases, staged at set-up
+            v[i] = val;
+        }
+        if (g.relu_mask) {
+            const float* mrow = g.relu_mask + (long long)m * g.ldm + nb;
+            if (full && g.vec_mask) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const float4 mk = reinterpret_cast<const float4*>(mrow)[q];
+                    if (!(mk.x > 0.f)) v[4 * q] = 0.f;
+                    if (!(mk.y > 0.f)) v[4 * q + 1] = 0.f;
+                    if (!(mk.z > 0.f)) v[4 * q + 2] = 0.f;
+                    if (!(mk.w > 0.f)) v[4 * q + 3] = 0.f;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (nb + i < g.N && !(mrow[i] > 0.f))
+                        v[i] = 0.f;
+            }
+        }
+        if (out_f) {
+            float* orow = out_f + (long long)m * g.ldo_f + nb;
+            if (full && g.vec_f) {
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    reinterpret_cast<float4*>(orow)[q] =
+                        make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (nb + i < g.N)
+                        orow[i] = v[i];
+            }
+        }
+        if (g.out_b) {
+            __nv_bfloat16* brow = g.out_b + (long long)m * g.ldo_b + nb;
+            if (full && g.vec_b) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    float b8[8];
+#pragma unroll
+                    for (int i = 0; i < 8; ++i)
+                        b8[i] = g.relu ? fmaxf(v[8 * q + i], 0.f) : v[8 * q + i];
+                    reinterpret_cast<uint4*>(brow)[q] = pack8(b8);
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (nb + i < g.N)
+                        brow[i] = __float2bfloat16_rn(g.relu ? fmaxf(v[i], 0.f) : v[i]);
+            }
+        }
+    }
+}
+
 // Two operand buffers: the K chunk after the current one is staged while
 // the tensor cores work on the current one; buffer b is refilled only after
 // the MMAs that read it have signalled its mbarrier.
@@ -235,8 +318,12 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ uint32_t tmem_slot;
     __shared__ int s_fail;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    __shared__ float s_bias[kBN];
+    const int tid = threadIdx.x, warp = tid >> 5;
     const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    if (g.bias)
+        for (int i = tid; i < kBN; i += blockDim.x)
+            s_bias[i] = n0 + i < g.N ? g.bias[n0 + i] : 0.f;
     if (warp == 0)
         umma::tmem_alloc(&tmem_slot, 256);
     if (tid == 0) {
@@ -304,85 +391,123 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(GemmArgs g) {
     umma::fence_after_sync();
     const bool empty = kbeg >= nk;  // this split has no K chunk: its partial is zero
     if (!s_fail) {
-        const int quarter = warp & 3, half = warp >> 2;
-        const int m = m0 + quarter * 32 + lane;
-        for (int c = half * (kBN / 64); c < (half + 1) * (kBN / 64); ++c) {
-            float v[32];
-            umma::tmem_ld32(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(c * 32), v);
-            if (m >= g.M)
-                continue;
-            if (empty)
-#pragma unroll
-                for (int i = 0; i < 32; ++i)
-                    v[i] = 0.f;
-            // 32 consecutive outputs of row m: 16-byte vector loads and stores
-            // where the host found the rows aligned, element by element else
-            const int nb = n0 + c * 32;
-            const bool full = nb + 31 < g.N;
-#pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                float val = v[i] * g.scale;
-                if (g.bias && nb + i < g.N)
-                    val += g.bias[nb + i];
-                v[i] = val;
-            }
-            if (g.relu_mask) {
-                const float* mrow = g.relu_mask + (long long)m * g.ldm + nb;
-                if (full && g.vec_mask) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const float4 mk = reinterpret_cast<const float4*>(mrow)[q];
-                        if (!(mk.x > 0.f)) v[4 * q] = 0.f;
-                        if (!(mk.y > 0.f)) v[4 * q + 1] = 0.f;
-                        if (!(mk.z > 0.f)) v[4 * q + 2] = 0.f;
-                        if (!(mk.w > 0.f)) v[4 * q + 3] = 0.f;
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i)
-                        if (nb + i < g.N && !(mrow[i] > 0.f))
-                            v[i] = 0.f;
-                }
-            }
-            if (out_f) {
-                float* orow = out_f + (long long)m * g.ldo_f + nb;
-                if (full && g.vec_f) {
-#pragma unroll
-                    for (int q = 0; q < 8; ++q)
-                        reinterpret_cast<float4*>(orow)[q] =
-                            make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i)
-                        if (nb + i < g.N)
-                            orow[i] = v[i];
-                }
-            }
-            if (g.out_b) {
-                __nv_bfloat16* brow = g.out_b + (long long)m * g.ldo_b + nb;
-                if (full && g.vec_b) {
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        float b8[8];
-#pragma unroll
-                        for (int i = 0; i < 8; ++i)
-                            b8[i] = g.relu ? fmaxf(v[8 * q + i], 0.f) : v[8 * q + i];
-                        reinterpret_cast<uint4*>(brow)[q] = pack8(b8);
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i)
-                        if (nb + i < g.N)
-                            brow[i] = __float2bfloat16_rn(g.relu ? fmaxf(v[i], 0.f) : v[i]);
-                }
-            }
-        }
+        gemm_epilogue(g, tmem, m0, n0, empty, out_f, g.bias ? s_bias : nullptr);
     } else {
         if (tid == 0)
             atomicExch(g.err, 1);
         // let the MMAs in flight finish (bounded) before the TMEM is released
         if (last >= 0)
             umma::mbar_wait(umma::smem_u32(&mbar[last & 1]), parity_of(last), kWaitLimit);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) {
+        umma::fence_after_sync();
+        umma::tmem_dealloc(tmem, 256);
+    }
+}
+
+// TMA-fed GEMM for BF16 operands whose rows are K-contiguous (the forward
+// GEMMs: activations or features times the BF16 weight copy): a 4-stage ring
+// of 128 x 64 (A) and 256 x 64 (B) tiles that the Tensor Memory Accelerator
+// writes with 128-byte swizzling (cp.async.bulk.tensor, tensor maps over this
+// GPU's memory, no multicast), one producer thread, one MMA thread
+// (tcgen05.mma reading the swizzled tiles directly), the same epilogue.
+// full[s] completes when a stage's two tiles have landed, empty[s] when the
+// MMAs that read it are done; every wait is bounded.
+constexpr int kTmaStages = 4;
+constexpr int kTmaTileA = kBM * kBK * 2, kTmaTileB = kBN * kBK * 2;
+constexpr size_t kTmaSmem = 1024 + (size_t)kTmaStages * (kTmaTileA + kTmaTileB);
+constexpr uint32_t kTmaWaitLimit = 1u << 20;
+
+__global__ void __launch_bounds__(kGemmThreads, 1)
+    gemm_tma_kernel(const __grid_constant__ CUtensorMap tma_a,
+                    const __grid_constant__ CUtensorMap tma_b, GemmArgs g) {
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    unsigned char* smem = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
+    __shared__ __align__(8) uint64_t full[kTmaStages], empty[kTmaStages], done;
+    __shared__ uint32_t tmem_slot;
+    __shared__ int s_fail, s_issued, s_consumed;
+    __shared__ float s_bias[kBN];
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    if (g.bias)
+        for (int i = tid; i < kBN; i += blockDim.x)
+            s_bias[i] = n0 + i < g.N ? g.bias[n0 + i] : 0.f;
+    if (warp == 0)
+        umma::tmem_alloc(&tmem_slot, 256);
+    if (tid == 0) {
+        for (int i = 0; i < kTmaStages; ++i) {
+            umma::mbar_init(umma::smem_u32(&full[i]), 1);
+            umma::mbar_init(umma::smem_u32(&empty[i]), 1);
+        }
+        umma::mbar_init(umma::smem_u32(&done), 1);
+        s_fail = 0;
+        s_issued = 0;
+        s_consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tmem_slot;
+    const int nk = g.K / kBK;
+    auto sA = [&](int st) { return smem + st * (kTmaTileA + kTmaTileB); };
+    auto sB = [&](int st) { return smem + st * (kTmaTileA + kTmaTileB) + kTmaTileA; };
+    if (tid == 0) {  // producer
+        int kb = 0;
+        for (; kb < nk; ++kb) {
+            const int st = kb % kTmaStages;
+            if (kb >= kTmaStages &&
+                !umma::mbar_wait(umma::smem_u32(&empty[st]), ((kb / kTmaStages) - 1) & 1,
+                                 kTmaWaitLimit)) {
+                atomicExch(&s_fail, 1);
+                break;
+            }
+            if (*(volatile int*)&s_fail)
+                break;
+            const uint32_t fb = umma::smem_u32(&full[st]);
+            umma::mbar_arrive_expect_tx(fb, kTmaTileA + kTmaTileB);
+            umma::tma_load_2d(umma::smem_u32(sA(st)), &tma_a, kb * kBK, m0, fb);
+            umma::tma_load_2d(umma::smem_u32(sB(st)), &tma_b, kb * kBK, n0, fb);
+        }
+        s_issued = kb;
+    } else if (tid == 32) {  // MMA issuer
+        const uint32_t idesc = umma::idesc_bf16(kBM, kBN);
+        int kb = 0;
+        for (; kb < nk; ++kb) {
+            const int st = kb % kTmaStages;
+            if (!umma::mbar_wait(umma::smem_u32(&full[st]), (kb / kTmaStages) & 1,
+                                 kTmaWaitLimit)) {
+                atomicExch(&s_fail, 1);
+                break;
+            }
+            umma::fence_after_sync();
+            const uint32_t a0 = umma::smem_u32(sA(st)), b0 = umma::smem_u32(sB(st));
+#pragma unroll
+            for (int s = 0; s < kBK / 16; ++s)
+                umma::mma_bf16(tmem, umma::smem_desc_sw128(a0 + s * 32),
+                               umma::smem_desc_sw128(b0 + s * 32), idesc,
+                               (kb > 0 || s > 0) ? 1u : 0u);
+            umma::commit(umma::smem_u32(&empty[st]));
+        }
+        s_consumed = kb;
+        // arrives once every MMA issued above has completed
+        umma::commit(umma::smem_u32(&done));
+    }
+    __syncthreads();
+    const bool ok = !s_fail && umma::mbar_wait(umma::smem_u32(&done), 0, kTmaWaitLimit);
+    umma::fence_after_sync();
+    if (ok) {
+        gemm_epilogue(g, tmem, m0, n0, nk == 0, g.out_f, g.bias ? s_bias : nullptr);
+    } else if (tid == 0) {
+        atomicExch(g.err, 1);
+        // loads issued but never consumed still land in this CTA's shared
+        // memory: wait for them (bounded) before the CTA exits
+        for (int kb = s_consumed; kb < s_issued; ++kb)
+            umma::mbar_wait(umma::smem_u32(&full[kb % kTmaStages]), (kb / kTmaStages) & 1,
+                            kTmaWaitLimit);
     }
     umma::fence_before_sync();
     __syncthreads();
@@ -540,6 +665,48 @@ int stage_mode(const void* p, int bf16, long long ld_r, long long ld_k) {
     return kStageElem;
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+// 2-D BF16 tensor map of `rows` rows of K elements (row pitch `row_bytes`),
+// boxes of 64 x box_rows, 128-byte swizzle, zero fill outside the matrix.
+bool make_bf16_map(CUtensorMap* m, const void* base, long long K, long long rows,
+                   long long row_bytes, int box_rows) {
+    const auto encode = tensor_map_encoder();
+    if (!encode)
+        return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+    const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
+                  box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+int g_mlp_use_tma = 1;
+
+namespace {
+
 int gemm_launch(const GemmArgs& a, cudaStream_t s) {
     static thread_local int attr_dev = -1;
     int dev = -1;
@@ -547,6 +714,9 @@ int gemm_launch(const GemmArgs& a, cudaStream_t s) {
     if (attr_dev != dev) {
         BMM_CUDA_TRY(cudaFuncSetAttribute(gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)kGemmSmem));
+        BMM_CUDA_TRY(cudaFuncSetAttribute(gemm_tma_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)kTmaSmem));
         attr_dev = dev;
     }
     GemmArgs g = a;
@@ -558,6 +728,20 @@ int gemm_launch(const GemmArgs& a, cudaStream_t s) {
     g.vec_b = a.out_b && al16(a.out_b) && a.ldo_b % 8 == 0;
     g.vec_mask = a.relu_mask && al16(a.relu_mask) && a.ldm % 4 == 0;
     dim3 grid((a.M + kBM - 1) / kBM, (a.N + kBN - 1) / kBN, a.ksplit > 1 ? a.ksplit : 1);
+    // BF16 operands with K-contiguous, 16-byte aligned rows and whole 64-wide
+    // K chunks: TMA staging (box x coordinates are multiples of 64 elements)
+    if (g_mlp_use_tma && a.a_bf16 && a.b_bf16 && g.a_mode == kStageKVec &&
+        g.b_mode == kStageKVec && a.K % kBK == 0 && a.ksplit <= 1) {
+        CUtensorMap ma, mb;
+        if (make_bf16_map(&ma, a.A, a.K, a.M, a.lda_m * 2, kBM) &&
+            make_bf16_map(&mb, a.B, a.K, a.N, a.ldb_n * 2, kBN)) {
+            gemm_tma_kernel<<<grid, kGemmThreads, kTmaSmem, s>>>(ma, mb, g);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess)
+                return fail(BMM_ECUDA, "mlp: gemm (TMA) launch failed: %s", cudaGetErrorString(e));
+            return BMM_OK;
+        }
+    }
     gemm_kernel<<<grid, kGemmThreads, kGemmSmem, s>>>(g);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
@@ -652,11 +836,13 @@ namespace mlp {
 
 // Forward pass of `rows` inputs X (FP32 or BF16, row stride kIn) into the
 // handle's scratch: z1/h1, z2/h2, logits z3 (or `logits` if given).
-int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) {
+int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits, bool keep_pre) {
+    // keep_pre: also write the FP32 pre-activations z1, z2 (the ReLU masks of
+    // a following backward pass); inference needs only the BF16 activations
     GemmArgs a = gemm_args(X, x_bf16, kIn, 1, h->wb + kW1, 1, kIn, 1, rows, kHid, kIn, h->err);
     a.bias = h->w + kB1;
     a.relu = 1;
-    a.out_f = h->z1;
+    a.out_f = keep_pre ? h->z1 : nullptr;
     a.ldo_f = kHid;
     a.out_b = h->h1;
     a.ldo_b = kHid;
@@ -664,7 +850,7 @@ int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits) 
     a = gemm_args(h->h1, 1, kHid, 1, h->wb + kW2, 1, kHid, 1, rows, kHid, kHid, h->err);
     a.bias = h->w + kB2;
     a.relu = 1;
-    a.out_f = h->z2;
+    a.out_f = keep_pre ? h->z2 : nullptr;
     a.ldo_f = kHid;
     a.out_b = h->h2;
     a.ldo_b = kHid;
@@ -926,9 +1112,26 @@ BMM_API int bmm_mlp_forward_dev(bmm_mlp* h, const float* x, size_t rows, float* 
     if (rows > (1u << 24))
         return fail(BMM_EINVAL, "mlp: too many rows");
     BMM_TRY(ensure_cap(h, rows));
-    BMM_TRY(forward_dev(h, x, 0, (int)rows, nullptr));
-    BMM_CUDA_TRY(cudaMemcpyAsync(logits, h->z3, rows * kOut * 4, cudaMemcpyDeviceToDevice,
-                                 h->stream));
+    return forward_dev(h, x, 0, (int)rows, logits, false);
+}
+
+BMM_API int bmm_mlp_forward_bf16_dev(bmm_mlp* h, const void* x, size_t rows, float* logits) {
+    clear_error();
+    if (!h || (rows && (!x || !logits)))
+        return fail(BMM_EINVAL, "mlp: null argument");
+    if (rows == 0)
+        return BMM_OK;
+    if (rows > (1u << 24))
+        return fail(BMM_EINVAL, "mlp: too many rows");
+    BMM_TRY(ensure_cap(h, rows));
+    return forward_dev(h, x, 1, (int)rows, logits, false);
+}
+
+BMM_API int bmm_mlp_tune(int use_tma) {
+    clear_error();
+    if (use_tma != 0 && use_tma != 1)
+        return fail(BMM_EINVAL, "mlp tuning: use_tma must be 0 or 1");
+    g_mlp_use_tma = use_tma;
     return BMM_OK;
 }
 

@@ -55,7 +55,8 @@ int create(uint64_t seed, float learning_rate, cudaStream_t stream, bmm_mlp** ou
 void destroy(bmm_mlp* h);
 // rows inputs X [rows][512] (BF16 if x_bf16, else FP32) -> logits [rows][256]
 // (h->z3 when logits is null); asynchronous on h->stream.
-int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits);
+int forward_dev(bmm_mlp* h, const void* X, int x_bf16, int rows, float* logits,
+                bool keep_pre = true);
 // One Adam step on targets T [rows][256]; the loss goes to *h->loss.
 int train_step_dev(bmm_mlp* h, const void* X, int x_bf16, const float* T, int rows);
 int ensure_cap(bmm_mlp* h, size_t rows);

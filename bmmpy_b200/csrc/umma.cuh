@@ -20,6 +20,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, uint32_t lbo, uint
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// Shared-memory descriptor of a K-major operand tile written by TMA with
+// 128-byte swizzling: rows of 64 BF16 (128 bytes), 8-row atoms of 1024 bytes
+// (stride byte offset 1024), leading byte offset unused (1), layout type
+// SWIZZLE_128B (2 in bits 61-63).  The tile base must be 1024-byte aligned;
+// the K step of 16 elements inside the atom is +32 bytes of start address.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+           (1ull << 46) | (2ull << 61);
+}
+
 // Instruction descriptor, kind::f16: FP32 accumulate, BF16 A and B, both
 // K-major, shape M x N.
 __host__ __device__ constexpr uint32_t idesc_bf16(int M, int N) {
@@ -66,6 +76,26 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint32
             return true;
     }
     return false;
+}
+
+// The mbarrier's next phase completes after one arrival plus `bytes` of
+// asynchronous (TMA) transfers.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t mbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes)
+                 : "memory");
+}
+
+// 2-D tiled TMA load of the box at (x, y) (x: innermost coordinate, a
+// multiple of 8 BF16 elements = 16 bytes) into shared memory, completing
+// transaction bytes on `mbar`.  The tensor map covers this GPU's memory only
+// and no multicast is used.
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const void* tmap, int x, int y,
+                                            uint32_t mbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+        "[%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(mbar)
+        : "memory");
 }
 
 __device__ __forceinline__ void fence_async_smem() {

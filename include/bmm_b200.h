@@ -418,6 +418,12 @@ BMM_API int bmm_mlp_create_on_stream(uint64_t seed, float learning_rate, void* s
 BMM_API int bmm_mlp_forward_dev(bmm_mlp* h, const float* x, size_t rows, float* logits);
 BMM_API int bmm_mlp_train_dev(bmm_mlp* h, const float* x, const float* target, size_t rows,
                               int steps);
+/* forward_dev with BF16 inputs x [rows][512] (the GA's proposal features). */
+BMM_API int bmm_mlp_forward_bf16_dev(bmm_mlp* h, const void* x, size_t rows, float* logits);
+/* GEMM operand staging: 1 (default) = TMA (cp.async.bulk.tensor, 4-stage
+ * ring) for BF16 operands with K-contiguous rows, 0 = thread staging for
+ * every GEMM.  Results are the same; only speed differs. */
+BMM_API int bmm_mlp_tune(int use_tma);
 
 /* ---- exact minimum-weight basis of a window ------------------------------
  * ExactBasisSolverConfig / ExactBasisResult of
