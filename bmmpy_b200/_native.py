@@ -160,6 +160,8 @@ SIGNATURES = {
     "bmm_spectrum_low_bits": [_sz],
     "bmm_spectrum_topk_slices_dev": [_vp, _sz, _sz, _sz, _sz, C.c_int, C.c_int64, C.c_int64, _vp,
                                      _vp],
+    "bmm_split_window_dev": [_vp, _sz, _sz, _sz, _sz, _vp, _vp, _vp, _sz, _szp,
+                             C.POINTER(C.c_int32), _vp],
     "bmm_last_error": [],
     "bmm_version": [],
     "bmm_runtime_features": [C.POINTER(Features_t)],

@@ -608,6 +608,22 @@ BMM_API int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_
                                          size_t k, int low_bits, int64_t slice_begin,
                                          int64_t slice_end, bmm_candidate* d_out, void* stream);
 
+/* ---- split-window preparation on the device ----------------------------
+ * build_compact_split_window (include/bmmpy/search/split_window_prep.hpp:21-26,
+ * src/search/split_window_prep.cpp:42-137) over the t rows d_rows (device,
+ * t x W words, W >= ceil(cols / 64); bits past cols are ignored): the
+ * distinct nonzero t-bit column patterns (bit i = row i) in ascending order,
+ * written as d_q[i] = pattern >> low_bits, d_r[i] = pattern & (2^low_bits - 1)
+ * and d_mult[i] = its column count, for i < *n_unique; *total_weight = the
+ * number of active columns.  cap = the room in d_q / d_r / d_mult (cols
+ * always suffices); more distinct patterns than cap is BMM_EINVAL.  The
+ * reference's checks and messages: low_bits > t, t > 64.  Synchronises
+ * `stream` (the counts are returned on the host). */
+BMM_API int bmm_split_window_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols,
+                                 size_t low_bits, uint64_t* d_q, uint64_t* d_r, int32_t* d_mult,
+                                 size_t cap, size_t* n_unique, int32_t* total_weight,
+                                 void* stream);
+
 /* Autotuner hook for the enumeration kernel (no reference counterpart):
  * carry-save blocks of 8 words per 64-word lane (0, 2, 5 or 8; -1 = built-in
  * policy).  Process-wide; results never change, only speed. */
