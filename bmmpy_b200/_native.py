@@ -154,6 +154,7 @@ SIGNATURES = {
     "bmm_gray_tune_lanes": [C.c_int],
     "bmm_spectrum_tune": [C.c_int],
     "bmm_spectrum_tune_last_pass": [C.c_int],
+    "bmm_spectrum_tune_passes": [C.c_int],
     "bmm_gray_tune_shape": [_sz, _sz, C.c_int, C.c_int, C.c_int],
     "bmm_spectrum_tune_shape": [_sz, C.c_int],
     "bmm_tune_reset": [],

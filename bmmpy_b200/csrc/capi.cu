@@ -683,6 +683,14 @@ int bmm_spectrum_tune_last_pass(int double_buffered) {
     return BMM_OK;
 }
 
+int bmm_spectrum_tune_passes(int register_resident) {
+    clear_error();
+    if (register_resident != 0 && register_resident != 1)
+        return fail(BMM_EINVAL, "spectrum tuning: register_resident must be 0 or 1");
+    g_spectrum_reg = register_resident;
+    return BMM_OK;
+}
+
 int bmm_spectrum_low_bits(size_t t) { return t > 40 ? -1 : spectrum_low_bits((int)t); }
 
 int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols, size_t k,

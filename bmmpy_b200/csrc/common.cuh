@@ -51,6 +51,7 @@ enum Slot : int {
     kSlotSweepNew,
     kSlotSweepState,
     kSlotSweepOrder,
+    kSlotEmptyBits,   // spectrum: one bit per pass-A tile without patterns
     kSlotCount
 };
 

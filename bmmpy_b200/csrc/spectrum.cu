@@ -15,16 +15,18 @@
 //       sparse histogram is never written; empty tiles (all-zero transforms)
 //       are not written at all, and the next pass zero-fills their rows from
 //       the bucket offsets instead of reading them;
-//   middle passes (<= 9 bits, 32 consecutive elements per row so every warp
-//       access is a full 128-byte line): read, transform, write;
+//   middle passes (<= 9 bits, >= 32 consecutive elements per row so every
+//       warp access is a full 128-byte line): read, transform, write;
 //   the last pass keeps its values in registers and feeds the weight + top-k
 //       scan instead of writing (warp-register top-k lists, merged at the end).
 // For t > 33 the extra high bits are enumerated (meet-in-the-middle): slice x
 // transforms the low 33 bits of the histogram signed by parity(high & x).
 // Traffic for t = 32: write 16 GB x (share of nonempty pass-A tiles) + read
 // the same + write 16 GB + read 16 GB (64 GB when every tile is nonempty).
-// The middle / last passes move tiles with 16-byte cp.async; a source size
-// of 0 zero-fills without a read.
+// Passes of 6..9 bits (k <= 128) load HBM straight into registers and
+// exchange once through shared memory (pass_reg_kernel); narrower passes and
+// k > 128 move tiles with 16-byte cp.async (pass_mid_kernel), where a source
+// size of 0 zero-fills without a read.
 #include "common.cuh"
 #include "spectrum.cuh"
 #include "topk.cuh"
@@ -443,6 +445,236 @@ __global__ void __launch_bounds__(kThr, (LAST && DB) ? 1 : 2)
                         cta_out + (size_t)blockIdx.x * kk);
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident passes (6 <= R <= 9 row bits, tiles of 2^R rows x 2^B
+// consecutive entries, B = 14 - R >= 5).  Lane = column within a 32-column
+// block, so every warp load or store of one row is one full 128-byte line,
+// and values go from HBM straight into registers:
+//   round 1: element e of a thread is row e | rw << 6 (the six low row bits
+//            in registers, six stages with no shared memory);
+//   round 2 (R > 6): one exchange through shared memory, laid out row-major
+//            (lane = column: conflict-free without a swizzle), then the R - 6
+//            high row stages in registers.
+// 8 bytes per value cross shared memory (the cp.async passes move 16-20).
+// The next tile's loads are issued into a second register set before the
+// current tile is transformed, so HBM reads overlap the whole tile.  Each
+// add of a butterfly is an IMAD (x * one + y, `one` == 1 at run time) on the
+// FMA pipe and each subtract an IADD on the ALU pipe.
+template <int R>
+struct RegTile {
+    static constexpr int B = kTileLog - R;  // log2 columns per row, 5..8
+    static constexpr int CWB = B - 5;       // warp bits choosing the 32-column block
+    static constexpr int RWB = R - 6;       // warp bits choosing row bits (both rounds)
+    static_assert(R >= 6 && R <= 9, "register passes take 6..9 row bits");
+    // row of element e = the e part | the warp part
+    __device__ static __forceinline__ int row1_e(int e) { return e; }
+    __device__ static __forceinline__ int row1_w(int rw) { return rw << 6; }
+    __device__ static __forceinline__ int row2_e(int e) {
+        return (e >> RWB) | ((e & ((1 << RWB) - 1)) << 6);
+    }
+    __device__ static __forceinline__ int row2_w(int rw) { return rw << (12 - R); }
+    __device__ static __forceinline__ int row1(int e, int rw) { return row1_e(e) | row1_w(rw); }
+    __device__ static __forceinline__ int row2(int e, int rw) { return row2_e(e) | row2_w(rw); }
+    __device__ static __forceinline__ int last_e(int e) { return R > 6 ? row2_e(e) : row1_e(e); }
+    __device__ static __forceinline__ int last_w(int rw) { return R > 6 ? row2_w(rw) : row1_w(rw); }
+    __device__ static __forceinline__ int row_last(int e, int rw) { return last_e(e) | last_w(rw); }
+};
+
+// Byte stride between rows, 4 << lo < 2^32 (lo <= 27), read through an asm
+// move so that the compiler forms each address in the tile loop (one wide
+// IMAD) instead of keeping 64 loop-invariant 64-bit offsets in registers.
+__device__ __forceinline__ uint32_t row_stride_bytes(int lo) {
+    uint32_t sb;
+    asm volatile("mov.b32 %0, %1;" : "=r"(sb) : "r"(4u << lo));
+    return sb;
+}
+
+__device__ __forceinline__ uint32_t mad_one(uint32_t a, uint32_t one, uint32_t c) {
+    uint32_t d;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(one), "r"(c));
+    return d;
+}
+
+template <int S0, int NS>
+__device__ __forceinline__ void bfly_split(int32_t (&x)[64], uint32_t one) {
+#pragma unroll
+    for (int s = S0; s < S0 + NS; ++s) {
+#pragma unroll
+        for (int e = 0; e < 64; ++e)
+            if ((e & (1 << s)) == 0) {
+                const uint32_t u = (uint32_t)x[e], v = (uint32_t)x[e | (1 << s)];
+                x[e] = (int32_t)mad_one(v, one, u);
+                x[e | (1 << s)] = (int32_t)(u - v);
+            }
+    }
+}
+
+// Offer a tile's 64 register values (rows row_last(e), column col) to the
+// warp top-k.  Values above `lim` = min(own threshold, *gthr) are dropped:
+// *gthr is the smallest threshold weight any warp of the launch has published,
+// i.e. some warp holds k candidates of at most that weight, so a value above
+// it is not among the k best of the window (values at or below it are always
+// offered, and each warp's list keeps the k best it was offered, so the merged
+// lists stay exact).  The prefilter is one integer max per value (N - WHT is
+// even and in [0, 2N]); when some lane may pass it, the thread parks its
+// values at its own shared-memory positions (no other thread touches them
+// before the next barrier) and walks them in a rolled loop, one warp vote per
+// value, offering only where a lane is at or below the limit.
+template <int R, int E>
+__device__ __forceinline__ void reg_offer(const int32_t (&x)[64], int rw, int col, uint64_t mbase,
+                                          int lo, long long N, int kk, WarpTopK<E>& top,
+                                          uint32_t& thr, int32_t* s, unsigned* gthr) {
+    using M = RegTile<R>;
+    uint32_t g;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(g) : "l"(gthr) : "memory");
+    uint32_t lim = min(thr, g);
+    if (N < (1ll << 30)) {
+        int32_t h8[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            h8[j] = x[j];
+#pragma unroll
+        for (int e = 8; e < 64; ++e)
+            h8[e & 7] = max(h8[e & 7], x[e]);
+        const int32_t hi = max(max(max(h8[0], h8[1]), max(h8[2], h8[3])),
+                               max(max(h8[4], h8[5]), max(h8[6], h8[7])));
+        const uint32_t lo2 = (uint32_t)N - (uint32_t)hi;
+        if (!__any_sync(kFull, (lo2 >> 1) <= lim))
+            return;
+    }
+#pragma unroll
+    for (int e = 0; e < 64; ++e)
+        s[(M::row_last(e, rw) << M::B) | col] = x[e];
+    const uint32_t thr0 = thr;
+    long long vmin = N - 2 * (long long)lim;  // weight <= lim  <=>  value >= vmin
+#pragma unroll 1
+    for (int e = 0; e < 64; ++e) {
+        const int row = M::row_last(e, rw);
+        const int32_t v = s[(row << M::B) | col];
+        if (!__any_sync(kFull, (long long)v >= vmin))
+            continue;
+        const uint64_t mask = mbase | ((uint64_t)row << lo);
+        const long long w2 = N - (long long)v;
+        const bool ok = mask != 0 && w2 >= 0 && (w2 & 1) == 0;
+        top.offer(ok, (uint32_t)(w2 >> 1), mask, kk, thr);
+        lim = min(thr, g);
+        vmin = N - 2 * (long long)lim;
+    }
+    if (thr < thr0 && (threadIdx.x & 31) == 0)
+        atomicMin(gthr, thr);
+}
+
+// One pass over the row bits [lo, lo + R).  empty_bits (first pass after
+// pass A only, lo == 14): bit i of word j set = pass-A tile 64 j + i was
+// never written; its rows are zeros and are not read.
+template <int R, bool LAST, int E>
+__global__ void __launch_bounds__(kThr, 1)
+    pass_reg_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
+                    const unsigned long long* __restrict__ total, int kk,
+                    bmm_candidate* __restrict__ cta_out, const uint64_t* __restrict__ empty_bits,
+                    unsigned* __restrict__ gthr, uint32_t one) {
+    using M = RegTile<R>;
+    constexpr int B = M::B;
+    extern __shared__ __align__(16) int32_t s[];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int cw = w & ((1 << M::CWB) - 1), rw = w >> M::CWB;
+    const int col = lane | (cw << 5);
+    const long long lowblocks = 1ll << (lo - B);
+    const long long ntiles = (1ll << T) >> kTileLog;
+    WarpTopK<E> top;
+    uint32_t thr = 0xffffffffu;
+    long long N = 0;
+    if (LAST) {
+        top.init();
+        N = (long long)*total;
+    }
+    auto tile_base = [&](long long tl) -> uint64_t {
+        return ((uint64_t)(tl / lowblocks) << (lo + R)) | ((uint64_t)(tl % lowblocks) << B);
+    };
+    auto load = [&](long long tl, int32_t (&x)[64]) {
+        const uint64_t gb = tile_base(tl);
+        uint64_t eb = 0;
+        if (empty_bits)
+            eb = __ldg(empty_bits + ((gb >> 20) | (uint64_t)rw));
+        const char* p = reinterpret_cast<const char*>(
+            d + (gb | ((uint64_t)M::row1_w(rw) << lo) | (uint64_t)col));
+        const uint32_t sb = row_stride_bytes(lo);
+        if (eb == 0) {  // warp-uniform: rw is one per warp
+#pragma unroll
+            for (int e = 0; e < 64; ++e)
+                x[e] = __ldcs(reinterpret_cast<const int32_t*>(
+                    p + (uint64_t)sb * (uint32_t)M::row1_e(e)));
+        } else {
+#pragma unroll
+            for (int e = 0; e < 64; ++e)
+                x[e] = ((eb >> e) & 1ull)
+                           ? 0
+                           : __ldcs(reinterpret_cast<const int32_t*>(
+                                 p + (uint64_t)sb * (uint32_t)M::row1_e(e)));
+        }
+    };
+    auto process = [&](long long tl, int32_t (&x)[64]) {
+        bfly_split<0, 6>(x, one);
+        if constexpr (R > 6) {
+            __syncthreads();  // the previous tile's round-2 reads are done
+#pragma unroll
+            for (int e = 0; e < 64; ++e)
+                s[(M::row1(e, rw) << B) | col] = x[e];
+            __syncthreads();
+#pragma unroll
+            for (int e = 0; e < 64; ++e)
+                x[e] = s[(M::row2(e, rw) << B) | col];
+            bfly_split<0, R - 6>(x, one);
+        }
+        const uint64_t gb = tile_base(tl);
+        if constexpr (LAST) {
+            reg_offer<R, E>(x, rw, col, (xhi << T) | gb | (uint64_t)col, lo, N, kk, top, thr,
+                            s, gthr);
+        } else {
+            char* p = reinterpret_cast<char*>(
+                d + (gb | ((uint64_t)M::last_w(rw) << lo) | (uint64_t)col));
+            const uint32_t sb = row_stride_bytes(lo);
+#pragma unroll
+            for (int e = 0; e < 64; ++e)
+                __stcs(reinterpret_cast<int32_t*>(p + (uint64_t)sb * (uint32_t)M::last_e(e)),
+                       x[e]);
+        }
+    };
+    const long long G = gridDim.x;
+    int32_t xa[64], xb[64];
+    long long tile = blockIdx.x;
+    if (tile < ntiles)
+        load(tile, xa);
+    while (tile < ntiles) {
+        const long long t1 = tile + G;
+        if (t1 < ntiles)
+            load(t1, xb);
+        process(tile, xa);
+        if (t1 >= ntiles)
+            break;
+        const long long t2 = t1 + G;
+        if (t2 < ntiles)
+            load(t2, xa);
+        process(t1, xb);
+        tile = t2;
+    }
+    if (LAST)
+        cta_list_out<E>(top, thr, kk, reinterpret_cast<bmm_candidate*>(s),
+                        cta_out + (size_t)blockIdx.x * kk);
+}
+
+// empty_bits[j] bit i = pass-A tile 64 j + i holds no pattern.
+__global__ void empty_bits_kernel(const unsigned* __restrict__ offsets, long long ntiles,
+                                  uint64_t* __restrict__ bits) {
+    const long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (j * 64 >= ntiles)
+        return;
+    uint64_t b = 0;
+    for (int i = 0; i < 64 && j * 64 + i < ntiles; ++i)
+        b |= (uint64_t)(offsets[j * 64 + i] == offsets[j * 64 + i + 1]) << i;
+    bits[j] = b;
+}
+
 // Small spectra (T < 14): one CTA, everything in shared memory.
 template <int E>
 __global__ void __launch_bounds__(kThr)
@@ -516,10 +748,44 @@ constexpr size_t mid_smem(bool last, int E, bool db = true) {
                 : kTile * sizeof(int32_t);
 }
 
+// Register-resident passes for R >= 6 row bits and lists of <= 128 entries
+// (WarpTopK<32> does not fit beside two register tiles).
+bool use_reg_pass(int R, int kk) { return g_spectrum_reg != 0 && R >= 6 && kk <= 128; }
+
+template <int E>
+int launch_reg(int R, bool last, int32_t* d, int T, int lo, unsigned long long xhi,
+               const unsigned long long* total, int kk, bmm_candidate* lists, int grid,
+               cudaStream_t st, const uint64_t* empty_bits, unsigned* gthr) {
+    const size_t smem = pass_smem(last, E);
+#define BMM_REG(RR)                                                                               \
+    case RR: {                                                                                    \
+        auto k = last ? pass_reg_kernel<RR, true, E> : pass_reg_kernel<RR, false, E>;             \
+        BMM_CUDA_TRY(                                                                             \
+            cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
+        k<<<grid, kThr, smem, st>>>(d, T, lo, xhi, total, kk, lists, empty_bits, gthr, 1u);       \
+        BMM_CUDA_TRY(cudaGetLastError());                                                         \
+        return BMM_OK;                                                                            \
+    }
+    switch (R) {
+        BMM_REG(6)
+        BMM_REG(7)
+        BMM_REG(8)
+        BMM_REG(9)
+    }
+#undef BMM_REG
+    return fail(BMM_EINVAL, "spectrum: bad pass width");
+}
+
 template <int E>
 int launch_mid(int R, bool last, int32_t* d, int T, int lo, unsigned long long xhi,
                const unsigned long long* total, int kk, bmm_candidate* lists, int grid,
-               cudaStream_t st, const unsigned* empty_offsets = nullptr) {
+               cudaStream_t st, const unsigned* empty_offsets = nullptr,
+               const uint64_t* empty_bits = nullptr, unsigned* gthr = nullptr) {
+    if constexpr (E <= 4) {
+        if (use_reg_pass(R, kk))
+            return launch_reg<E>(R, last, d, T, lo, xhi, total, kk, lists, grid, st, empty_bits,
+                                 gthr);
+    }
     const bool db = g_spectrum_last_db != 0 || E > 4;  // E = 32 lists need the registers
     const size_t smem = mid_smem(last, E, db);
 #define BMM_MID(RR)                                                                               \
@@ -562,10 +828,21 @@ int grid_for(Workspace* ws, long long ntiles) {
     return (int)(ntiles < g ? ntiles : g);
 }
 
+// Grid of a pass of width R after pass A: register passes and the
+// double-buffered last pass run one CTA per SM.
+int grid_mid(Workspace* ws, long long ntiles, int R, bool last, int kk) {
+    int per_sm = 2;
+    if (use_reg_pass(R, kk) || (last && (g_spectrum_last_db != 0 || kk > 128)))
+        per_sm = 1;
+    const long long g = (long long)ws->sm_count * per_sm;
+    return (int)(ntiles < g ? ntiles : g);
+}
+
 }  // namespace
 
 int g_spectrum_low_bits = -1;
 int g_spectrum_last_db = 1;
+int g_spectrum_reg = 1;
 int g_spectrum_shape_low_bits[41] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
                                      -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
                                      -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};
@@ -604,6 +881,9 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
     BMM_TRY(ws_buffer(ws, kSlotAux, (size_t)(cols > 0 ? cols : 1) * 8, &pats));
     BMM_TRY(ws_buffer(ws, kSlotCounter, 16, &cnt));
     BMM_CUDA_TRY(cudaMemsetAsync(cnt, 0, 8, stream));
+    // bytes 8..11: the smallest threshold weight published by the last pass
+    unsigned* gthr = reinterpret_cast<unsigned*>(static_cast<char*>(cnt) + 8);
+    BMM_CUDA_TRY(cudaMemsetAsync(gthr, 0xff, 4, stream));
     {
         long long blocks = (cols + 255) / 256;
         if (blocks > (long long)ws->sm_count * 8)
@@ -649,13 +929,17 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
         BMM_TRY(ws_buffer(ws, kSlotSpec, ((size_t)1 << T) * 4, &spec));
     int widths[4], nmid = 0;
     plan_mid(T, widths, &nmid);
-    const int grid_a = grid_for(ws, ntiles);
-    const int grid_m = grid_for(ws, ntiles);  // every pass has 2^(T-14) tiles
-    // the double-buffered last middle pass: one persistent CTA per SM
-    const int grid_last =
-        nmid ? (int)std::min<long long>(ntiles, (long long)ws->sm_count *
-                                                    (g_spectrum_last_db != 0 || kk > 128 ? 1 : 2))
-             : grid_a;
+    const int grid_a = grid_for(ws, ntiles);  // every pass has 2^(T-14) tiles
+    const int grid_last = nmid ? grid_mid(ws, ntiles, widths[nmid - 1], true, kk) : grid_a;
+    // pass-A tiles that hold no pattern, one bit each, for a register first pass
+    uint64_t* empty_bits = nullptr;
+    if (nmid && use_reg_pass(widths[0], kk)) {
+        const long long words = (ntiles + 63) / 64;
+        BMM_TRY(ws_buffer(ws, kSlotEmptyBits, (size_t)words * 8, (void**)&empty_bits));
+        empty_bits_kernel<<<(unsigned)((words + 255) / 256), 256, 0, stream>>>(
+            (const unsigned*)offsets, ntiles, empty_bits);
+        BMM_CUDA_TRY(cudaGetLastError());
+    }
     const long long slices = slice_end - slice_begin;
     bmm_candidate *lists = nullptr, *slice_lists = nullptr;
     BMM_TRY(ws_buffer(ws, kSlotCand, (size_t)grid_last * kk * sizeof(bmm_candidate),
@@ -690,10 +974,13 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
                 BMM_CUDA_TRY(cudaGetLastError());
                 int lo = kTileLog;
                 for (int i = 0; i < nmid; ++i) {
-                    BMM_TRY(launch_mid<E>(widths[i], i == nmid - 1, (int32_t*)spec, T, lo,
+                    const bool last = i == nmid - 1;
+                    BMM_TRY(launch_mid<E>(widths[i], last, (int32_t*)spec, T, lo,
                                           (unsigned long long)x, total, kk, lists,
-                                          i == nmid - 1 ? grid_last : grid_m, stream,
-                                          i == 0 ? (const unsigned*)offsets : nullptr));
+                                          last ? grid_last
+                                               : grid_mid(ws, ntiles, widths[i], false, kk),
+                                          stream, i == 0 ? (const unsigned*)offsets : nullptr,
+                                          i == 0 ? empty_bits : nullptr, gthr));
                     lo += widths[i];
                 }
             }
@@ -718,8 +1005,8 @@ int spectrum_dense_fwht(Workspace* ws, int32_t* d, int t, cudaStream_t stream) {
     plan_mid(t, widths, &nmid);
     int lo = kTileLog;
     for (int i = 0; i < nmid; ++i) {
-        BMM_TRY(launch_mid<1>(widths[i], false, d, t, lo, 0, nullptr, 0, nullptr,
-                              grid_for(ws, ntiles), stream));
+        BMM_TRY(launch_mid<1>(widths[i], false, d, t, lo, 0, nullptr, 1, nullptr,
+                              grid_mid(ws, ntiles, widths[i], false, 1), stream));
         lo += widths[i];
     }
     return BMM_OK;

@@ -112,3 +112,32 @@ def test_fwht_search_33_bits():
     assert got == sorted(got, key=lambda c: c.key())
     gray = bmm.BruteforceSearch(max_candidates=32).search(m.row_window(rows))
     assert as_pairs(got) == as_pairs(gray)
+
+
+@pytest.mark.parametrize("t,k,cols,density", [
+    (20, 64, 5000, 0.3), (21, 1, 777, 0.5), (23, 128, 20000, 0.05), (24, 64, 3000, 0.3),
+    (26, 5, 60000, 0.02), (29, 129, 4000, 0.4), (31, 64, 65536, 0.02),
+])
+def test_register_passes_match_tile_passes(t, k, cols, density):
+    """The register-resident transform passes (6..9 bits, k <= 128) against the
+    cp.async tile passes and, up to t = 26, the oracle: bit-exact top-k lists.
+    Windows with a sparse pattern set also exercise the empty-tile bits of the
+    first pass."""
+    from bmmpy_b200 import _native as N
+
+    P = port()
+    words, _ = P.gen_instance(t + 2, cols, density, 1000 + t, 3)
+    win = list(range(1, t + 1))
+    w = bmm.BitMatrix.from_words(words, cols).row_window(win)
+    s = bmm.MitmFwhtSearch(max_candidates=k)
+    lib = N.lib()
+    try:
+        N.check(lib.bmm_spectrum_tune_passes(0), "bmm_spectrum_tune_passes")
+        tiles = as_pairs(s.search(w))
+    finally:
+        N.check(lib.bmm_spectrum_tune_passes(1), "bmm_spectrum_tune_passes")
+    regs = as_pairs(s.search(w))
+    assert regs == tiles
+    if t <= 26:
+        assert regs == P.mitm_search(words, cols, win, k)
+    assert len(regs) == k
