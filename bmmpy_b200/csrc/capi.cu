@@ -685,8 +685,8 @@ int bmm_spectrum_tune_last_pass(int double_buffered) {
 
 int bmm_spectrum_tune_passes(int register_resident) {
     clear_error();
-    if (register_resident != 0 && register_resident != 1)
-        return fail(BMM_EINVAL, "spectrum tuning: register_resident must be 0 or 1");
+    if (register_resident < 0 || register_resident > 2)
+        return fail(BMM_EINVAL, "spectrum tuning: register_resident must be 0, 1 or 2");
     g_spectrum_reg = register_resident;
     return BMM_OK;
 }

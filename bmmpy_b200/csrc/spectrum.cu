@@ -456,8 +456,10 @@ __global__ void __launch_bounds__(kThr, (LAST && DB) ? 1 : 2)
 //            (lane = column: conflict-free without a swizzle), then the R - 6
 //            high row stages in registers.
 // 8 bytes per value cross shared memory (the cp.async passes move 16-20).
-// The next tile's loads are issued into a second register set before the
-// current tile is transformed, so HBM reads overlap the whole tile.  Each
+// Two CTAs per SM (one 64-value register tile per thread, <= 128 registers):
+// while one CTA waits on its loads the other transforms (measured faster than
+// one CTA per SM that prefetches the next tile into a second register set,
+// the PF variant).  Each
 // add of a butterfly is an IMAD (x * one + y, `one` == 1 at run time) on the
 // FMA pipe and each subtract an IADD on the ALU pipe.
 template <int R>
@@ -567,8 +569,8 @@ __device__ __forceinline__ void reg_offer(const int32_t (&x)[64], int rw, int co
 // One pass over the row bits [lo, lo + R).  empty_bits (first pass after
 // pass A only, lo == 14): bit i of word j set = pass-A tile 64 j + i was
 // never written; its rows are zeros and are not read.
-template <int R, bool LAST, int E>
-__global__ void __launch_bounds__(kThr, 1)
+template <int R, bool LAST, int E, bool PF = true>
+__global__ void __launch_bounds__(kThr, PF ? 1 : 2)
     pass_reg_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
                     const unsigned long long* __restrict__ total, int kk,
                     bmm_candidate* __restrict__ cta_out, const uint64_t* __restrict__ empty_bits,
@@ -641,6 +643,18 @@ __global__ void __launch_bounds__(kThr, 1)
         }
     };
     const long long G = gridDim.x;
+    if constexpr (!PF) {
+        // two CTAs per SM, one register tile each: the other CTA hides the loads
+        for (long long tile = blockIdx.x; tile < ntiles; tile += G) {
+            int32_t x[64];
+            load(tile, x);
+            process(tile, x);
+        }
+        if (LAST)
+            cta_list_out<E>(top, thr, kk, reinterpret_cast<bmm_candidate*>(s),
+                            cta_out + (size_t)blockIdx.x * kk);
+        return;
+    }
     int32_t xa[64], xb[64];
     long long tile = blockIdx.x;
     if (tile < ntiles)
@@ -759,7 +773,10 @@ int launch_reg(int R, bool last, int32_t* d, int T, int lo, unsigned long long x
     const size_t smem = pass_smem(last, E);
 #define BMM_REG(RR)                                                                               \
     case RR: {                                                                                    \
-        auto k = last ? pass_reg_kernel<RR, true, E> : pass_reg_kernel<RR, false, E>;             \
+        auto k = g_spectrum_reg == 2                                                              \
+                     ? (last ? pass_reg_kernel<RR, true, E, false>                                \
+                             : pass_reg_kernel<RR, false, E, false>)                              \
+                     : (last ? pass_reg_kernel<RR, true, E> : pass_reg_kernel<RR, false, E>);    \
         BMM_CUDA_TRY(                                                                             \
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
         k<<<grid, kThr, smem, st>>>(d, T, lo, xhi, total, kk, lists, empty_bits, gthr, 1u);       \
@@ -832,7 +849,9 @@ int grid_for(Workspace* ws, long long ntiles) {
 // double-buffered last pass run one CTA per SM.
 int grid_mid(Workspace* ws, long long ntiles, int R, bool last, int kk) {
     int per_sm = 2;
-    if (use_reg_pass(R, kk) || (last && (g_spectrum_last_db != 0 || kk > 128)))
+    if (use_reg_pass(R, kk))
+        per_sm = g_spectrum_reg == 2 ? 2 : 1;
+    else if (last && (g_spectrum_last_db != 0 || kk > 128))
         per_sm = 1;
     const long long g = (long long)ws->sm_count * per_sm;
     return (int)(ntiles < g ? ntiles : g);
@@ -842,7 +861,7 @@ int grid_mid(Workspace* ws, long long ntiles, int R, bool last, int kk) {
 
 int g_spectrum_low_bits = -1;
 int g_spectrum_last_db = 1;
-int g_spectrum_reg = 1;
+int g_spectrum_reg = 2;
 int g_spectrum_shape_low_bits[41] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
                                      -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1,
                                      -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1};

@@ -29,9 +29,10 @@ extern int g_spectrum_low_bits;
 // Last transform pass: 1 = one double-buffered CTA per SM, 0 = two
 // single-buffered CTAs per SM.
 extern int g_spectrum_last_db;
-// Passes of >= 6 row bits with lists of <= 128 entries: 1 = register-resident
-// (HBM straight to registers, one shared-memory exchange), 0 = the cp.async
-// tile passes.
+// Passes of >= 6 row bits with lists of <= 128 entries: register-resident
+// (HBM straight to registers, one shared-memory exchange) with 2 = two CTAs
+// per SM (default) or 1 = one CTA per SM prefetching the next tile into
+// registers; 0 = the cp.async tile passes.
 extern int g_spectrum_reg;
 // Per-t low bits found by the autotuner (bmm_spectrum_tune_shape); -1 = none.
 extern int g_spectrum_shape_low_bits[41];

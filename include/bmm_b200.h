@@ -603,10 +603,11 @@ BMM_API int bmm_spectrum_tune(int low_bits);
  * double-buffered CTA per SM (default), 0 = two single-buffered CTAs per SM.
  * Results never change, only speed. */
 BMM_API int bmm_spectrum_tune_last_pass(int double_buffered);
-/* Transform passes of 6..9 bits with k <= 128: 1 = register-resident
- * (default: HBM straight into registers, one shared-memory exchange per
- * tile, next tile prefetched into registers), 0 = the cp.async tile passes
- * (then bmm_spectrum_tune_last_pass applies).  Results never change. */
+/* Transform passes of 6..9 bits with k <= 128: register-resident (HBM
+ * straight into registers, one shared-memory exchange per tile) with
+ * 2 = two CTAs per SM (default) or 1 = one CTA per SM that prefetches the
+ * next tile into registers; 0 = the cp.async tile passes (then
+ * bmm_spectrum_tune_last_pass applies).  Results never change. */
 BMM_API int bmm_spectrum_tune_passes(int register_resident);
 BMM_API int bmm_spectrum_low_bits(size_t t);
 BMM_API int bmm_spectrum_topk_slices_dev(const uint64_t* d_rows, size_t t, size_t W, size_t cols,

@@ -134,10 +134,13 @@ def test_register_passes_match_tile_passes(t, k, cols, density):
     try:
         N.check(lib.bmm_spectrum_tune_passes(0), "bmm_spectrum_tune_passes")
         tiles = as_pairs(s.search(w))
-    finally:
         N.check(lib.bmm_spectrum_tune_passes(1), "bmm_spectrum_tune_passes")
+        prefetch = as_pairs(s.search(w))
+    finally:
+        N.check(lib.bmm_spectrum_tune_passes(2), "bmm_spectrum_tune_passes")
     regs = as_pairs(s.search(w))
     assert regs == tiles
+    assert prefetch == tiles
     if t <= 26:
         assert regs == P.mitm_search(words, cols, win, k)
     assert len(regs) == k
