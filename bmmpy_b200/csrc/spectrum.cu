@@ -40,6 +40,9 @@ constexpr int kTileLog = 14;
 constexpr int kTile = 1 << kTileLog;
 constexpr int kThr = 256;
 constexpr int kPer = kTile / kThr;  // 64
+// Pass-A tiles with at most this many patterns are written from the closed
+// form of their transform instead of being built and transformed.
+constexpr unsigned kDirectMax = 4;
 static_assert(kPer == 64, "register rounds assume 64 values per thread");
 
 __device__ __forceinline__ int swz(int k) { return k ^ ((k >> 6) & 31); }
@@ -206,49 +209,74 @@ __global__ void __launch_bounds__(1024) exclusive_scan_kernel(const unsigned* __
                                                               long long n,
                                                               unsigned* __restrict__ offsets,
                                                               unsigned* __restrict__ cursor) {
+    // Each thread owns a contiguous run of ceil(n / 1024) counts: it sums its
+    // run, one block-wide scan of the 1024 sums gives each run's start, and
+    // the thread writes its run's offsets (two barriers in all).
     __shared__ unsigned wsum[32];
-    __shared__ unsigned s_run;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0)
-        s_run = 0;
+    const long long per = (n + 1023) / 1024;
+    const long long b = min(n, (long long)tid * per), e = min(n, b + per);
+    const bool vec = (per & 3) == 0;  // runs start on 16-byte boundaries
+    unsigned sum = 0;
+    if (vec) {
+        const uint4* c4 = reinterpret_cast<const uint4*>(counts);
+#pragma unroll 8
+        for (long long i = b / 4; i < e / 4; ++i) {
+            const uint4 v = c4[i];
+            sum += v.x + v.y + v.z + v.w;
+        }
+    } else {
+        for (long long i = b; i < e; ++i)
+            sum += counts[i];
+    }
+    unsigned incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o)
+            incl += t;
+    }
+    if (lane == 31)
+        wsum[warp] = incl;
     __syncthreads();
-    for (long long c0 = 0; c0 < n; c0 += 1024) {
-        const long long i = c0 + tid;
-        const unsigned v = i < n ? counts[i] : 0u;
-        unsigned incl = v;
+    if (warp == 0) {
+        unsigned ws = wsum[lane];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const unsigned t = __shfl_up_sync(kFull, incl, o);
+            const unsigned t = __shfl_up_sync(kFull, ws, o);
             if (lane >= o)
-                incl += t;
+                ws += t;
         }
-        if (lane == 31)
-            wsum[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            unsigned ws = wsum[lane];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned t = __shfl_up_sync(kFull, ws, o);
-                if (lane >= o)
-                    ws += t;
-            }
-            wsum[lane] = ws;  // inclusive over warps
+        wsum[lane] = ws;  // inclusive over warps
+    }
+    __syncthreads();
+    unsigned run = (warp ? wsum[warp - 1] : 0u) + incl - sum;
+    if (vec) {
+        const uint4* c4 = reinterpret_cast<const uint4*>(counts);
+        uint4* o4 = reinterpret_cast<uint4*>(offsets);
+        uint4* u4 = reinterpret_cast<uint4*>(cursor);
+#pragma unroll 4
+        for (long long i = b / 4; i < e / 4; ++i) {
+            const uint4 v = c4[i];
+            uint4 o;
+            o.x = run;
+            o.y = o.x + v.x;
+            o.z = o.y + v.y;
+            o.w = o.z + v.z;
+            run = o.w + v.w;
+            o4[i] = o;
+            u4[i] = o;
         }
-        __syncthreads();
-        const unsigned run = s_run;
-        const unsigned excl = run + (warp ? wsum[warp - 1] : 0u) + incl - v;
-        if (i < n) {
-            offsets[i] = excl;
-            cursor[i] = excl;
+    } else {
+        for (long long i = b; i < e; ++i) {
+            const unsigned v = counts[i];
+            offsets[i] = run;
+            cursor[i] = run;
+            run += v;
         }
-        __syncthreads();
-        if (tid == 0)
-            s_run = run + wsum[31];
-        __syncthreads();
     }
     if (tid == 0)
-        offsets[n] = s_run;
+        offsets[n] = wsum[31];
 }
 
 __global__ void tile_scatter_kernel(const uint64_t* __restrict__ pats,
@@ -292,6 +320,40 @@ __global__ void __launch_bounds__(kThr, LAST ? 1 : 2)
             // the same offsets instead of reading them.
             if (b0 == b1 && !LAST)
                 continue;
+            if (!LAST && b1 - b0 <= kDirectMax) {
+                // A tile with few patterns: its transform in closed form,
+                // out[k] = sum_j v_j (-1)^popc(p_j & k), k = (e << 8) | tid,
+                // with no shared memory; the sign of element e is bit e of a
+                // 64-bit parity mask built from the pattern's bits 8..13.
+                int32_t x[64];
+#pragma unroll
+                for (int e = 0; e < 64; ++e)
+                    x[e] = 0;
+                for (unsigned i = b0; i < b1; ++i) {
+                    const uint64_t p = sorted[i];
+                    const int32_t v = (T < 64 && (__popcll((p >> T) & xhi) & 1)) ? -1 : 1;
+                    const uint32_t ph = (uint32_t)(p >> 8) & 63u;
+                    uint64_t m = 0;  // bit e = parity(ph & e) ^ parity(p & tid)
+                    if (ph & 1u) m ^= 0xAAAAAAAAAAAAAAAAull;
+                    if (ph & 2u) m ^= 0xCCCCCCCCCCCCCCCCull;
+                    if (ph & 4u) m ^= 0xF0F0F0F0F0F0F0F0ull;
+                    if (ph & 8u) m ^= 0xFF00FF00FF00FF00ull;
+                    if (ph & 16u) m ^= 0xFFFF0000FFFF0000ull;
+                    if (ph & 32u) m ^= 0xFFFFFFFF00000000ull;
+                    if (__popc((uint32_t)p & 255u & (uint32_t)tid) & 1)
+                        m = ~m;
+                    const uint32_t mlo = (uint32_t)m, mhi = (uint32_t)(m >> 32);
+#pragma unroll
+                    for (int e = 0; e < 64; ++e) {
+                        const uint32_t bit = ((e < 32 ? mlo : mhi) >> (e & 31)) & 1u;
+                        x[e] += bit ? -v : v;
+                    }
+                }
+#pragma unroll
+                for (int e = 0; e < 64; ++e)
+                    gt[(e << 8) | tid] = x[e];  // coalesced: consecutive tid
+                continue;
+            }
             int4* s4 = reinterpret_cast<int4*>(s);
             for (int i = tid; i < kTile / 4; i += kThr)
                 s4[i] = make_int4(0, 0, 0, 0);
