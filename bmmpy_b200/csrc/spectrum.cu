@@ -631,13 +631,17 @@ __device__ __forceinline__ void reg_offer(const int32_t (&x)[64], int rw, int co
 // One pass over the row bits [lo, lo + R).  empty_bits (first pass after
 // pass A only, lo == 14): bit i of word j set = pass-A tile 64 j + i was
 // never written; its rows are zeros and are not read.
-template <int R, bool LAST, int E, bool PF = true>
+// LO > 0: the pass's low bit is the compile-time LO (the first pass after
+// pass A has lo = 14): row addresses are then a base plus immediate offsets.
+template <int R, bool LAST, int E, bool PF = true, int LO = 0>
 __global__ void __launch_bounds__(kThr, PF ? 1 : 2)
     pass_reg_kernel(int32_t* __restrict__ d, int T, int lo, unsigned long long xhi,
                     const unsigned long long* __restrict__ total, int kk,
                     bmm_candidate* __restrict__ cta_out, const uint64_t* __restrict__ empty_bits,
                     unsigned* __restrict__ gthr, uint32_t one) {
     using M = RegTile<R>;
+    if constexpr (LO > 0)
+        lo = LO;
     constexpr int B = M::B;
     extern __shared__ __align__(16) int32_t s[];
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -662,7 +666,7 @@ __global__ void __launch_bounds__(kThr, PF ? 1 : 2)
             eb = __ldg(empty_bits + ((gb >> 20) | (uint64_t)rw));
         const char* p = reinterpret_cast<const char*>(
             d + (gb | ((uint64_t)M::row1_w(rw) << lo) | (uint64_t)col));
-        const uint32_t sb = row_stride_bytes(lo);
+        const uint32_t sb = LO > 0 ? (4u << LO) : row_stride_bytes(lo);
         if (eb == 0) {  // warp-uniform: rw is one per warp
 #pragma unroll
             for (int e = 0; e < 64; ++e)
@@ -697,7 +701,7 @@ __global__ void __launch_bounds__(kThr, PF ? 1 : 2)
         } else {
             char* p = reinterpret_cast<char*>(
                 d + (gb | ((uint64_t)M::last_w(rw) << lo) | (uint64_t)col));
-            const uint32_t sb = row_stride_bytes(lo);
+            const uint32_t sb = LO > 0 ? (4u << LO) : row_stride_bytes(lo);
 #pragma unroll
             for (int e = 0; e < 64; ++e)
                 __stcs(reinterpret_cast<int32_t*>(p + (uint64_t)sb * (uint32_t)M::last_e(e)),
@@ -837,7 +841,8 @@ int launch_reg(int R, bool last, int32_t* d, int T, int lo, unsigned long long x
     case RR: {                                                                                    \
         auto k = g_spectrum_reg == 2                                                              \
                      ? (last ? pass_reg_kernel<RR, true, E, false>                                \
-                             : pass_reg_kernel<RR, false, E, false>)                              \
+                             : (lo == kTileLog ? pass_reg_kernel<RR, false, E, false, kTileLog>   \
+                                               : pass_reg_kernel<RR, false, E, false>))           \
                      : (last ? pass_reg_kernel<RR, true, E> : pass_reg_kernel<RR, false, E>);    \
         BMM_CUDA_TRY(                                                                             \
             cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));     \
