@@ -124,7 +124,7 @@ int ws_pinned(Workspace* ws, size_t bytes, void** out) {
 }
 
 int merge_topk_lists(const bmm_candidate* d_lists, int nlists, int kk, bmm_candidate* d_out,
-                     cudaStream_t stream) {
+                     cudaStream_t stream, const unsigned* d_limit) {
     auto run = [&](auto Ec) -> int {
         constexpr int E = decltype(Ec)::value;
         auto mk = merge_lists_kernel<E>;
@@ -133,7 +133,7 @@ int merge_topk_lists(const bmm_candidate* d_lists, int nlists, int kk, bmm_candi
         const size_t msmem = (size_t)warps * 32 * E * sizeof(bmm_candidate);
         BMM_CUDA_TRY(
             cudaFuncSetAttribute(mk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)msmem));
-        mk<<<1, warps * 32, msmem, stream>>>(d_lists, nlists, kk, d_out);
+        mk<<<1, warps * 32, msmem, stream>>>(d_lists, nlists, kk, d_out, d_limit);
         BMM_CUDA_TRY(cudaGetLastError());
         return BMM_OK;
     };

@@ -1070,10 +1070,10 @@ int spectrum_topk_slices(Workspace* ws, const uint64_t* d_rows, int t, int W, lo
                     lo += widths[i];
                 }
             }
-            BMM_TRY(merge_topk_lists(lists, grid_last, kk, dst, stream));
+            BMM_TRY(merge_topk_lists(lists, grid_last, kk, dst, stream, gthr));
         }
         if (slices > 1)
-            BMM_TRY(merge_topk_lists(slice_lists, (int)slices, kk, d_out, stream));
+            BMM_TRY(merge_topk_lists(slice_lists, (int)slices, kk, d_out, stream, gthr));
         return BMM_OK;
     });
 }

@@ -118,14 +118,18 @@ struct WarpTopK {
     }
 };
 
-// Merge `nlists` sorted lists of kk entries into one top-kk list.
+// Merge `nlists` sorted lists of kk entries into one top-kk list.  limit
+// (optional): entries above *limit are known not to be among the kk best
+// (some list producer held kk entries of at most that weight) and are skipped.
 template <int E>
 __global__ void __launch_bounds__(1024) merge_lists_kernel(const bmm_candidate* __restrict__ lists,
                                                             int nlists, int kk,
-                                                            bmm_candidate* __restrict__ out) {
+                                                            bmm_candidate* __restrict__ out,
+                                                            const unsigned* __restrict__ limit) {
     extern __shared__ __align__(16) uint64_t smem_raw[];
     bmm_candidate* stage = reinterpret_cast<bmm_candidate*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t lim = limit ? *limit : 0xffffffffu;
     WarpTopK<E> top;
     top.init();
     uint32_t thr = 0xffffffffu;
@@ -137,7 +141,7 @@ __global__ void __launch_bounds__(1024) merge_lists_kernel(const bmm_candidate* 
             c.mask = ~0ull;
             if (j < kk)
                 c = lists[(size_t)l * kk + j];
-            const bool ok = c.weight != 0xffffffffu;
+            const bool ok = c.weight != 0xffffffffu && c.weight <= lim;
             if (!__any_sync(kFull, ok && c.weight <= thr))
                 break;
             top.offer(ok, c.weight, c.mask, kk, thr);
@@ -160,6 +164,6 @@ __global__ void __launch_bounds__(1024) merge_lists_kernel(const bmm_candidate* 
 
 // Host: merge `nlists` sorted device lists of kk entries into d_out (kk entries).
 int merge_topk_lists(const bmm_candidate* d_lists, int nlists, int kk, bmm_candidate* d_out,
-                     cudaStream_t stream);
+                     cudaStream_t stream, const unsigned* d_limit = nullptr);
 
 }  // namespace bmm
