@@ -71,3 +71,44 @@ def test_tuning_keeps_results(tmp_path, monkeypatch):
         assert A.apply_cached()["gray"]["24x3000k14"]["setting"] == g["setting"]
     finally:
         A.reset()
+
+
+def test_pass_knobs_are_checked():
+    """bmm_spectrum_tune_passes / _last_pass accept their documented values only
+    (host-side settings; nothing runs on the device)."""
+    L = N.lib()
+    try:
+        for v in (0, 1, 2):
+            N.check(L.bmm_spectrum_tune_passes(v))
+        for bad in (-1, 3, 7):
+            with pytest.raises(ValueError):
+                N.check(L.bmm_spectrum_tune_passes(bad))
+        for v in (0, 1):
+            N.check(L.bmm_spectrum_tune_last_pass(v))
+        with pytest.raises(ValueError):
+            N.check(L.bmm_spectrum_tune_last_pass(2))
+    finally:
+        N.check(L.bmm_spectrum_tune_passes(2))
+        N.check(L.bmm_spectrum_tune_last_pass(1))
+
+
+def test_split_window_c_abi_checks_before_device_work():
+    """bmm_split_window_dev: the reference's argument checks, in its order, and
+    the empty cases, all answered on the host."""
+    import ctypes as C
+
+    L = N.lib()
+    n = C.c_size_t(7)
+    tw = C.c_int32(7)
+    with pytest.raises(ValueError, match="low_bits must be <= number of rows"):
+        N.check(L.bmm_split_window_dev(None, 2, 1, 10, 3, None, None, None, 0, C.byref(n),
+                                       C.byref(tw), None))
+    with pytest.raises(ValueError, match="row count must be <= 64"):
+        N.check(L.bmm_split_window_dev(None, 65, 1, 10, 2, None, None, None, 0, C.byref(n),
+                                       C.byref(tw), None))
+    N.check(L.bmm_split_window_dev(None, 0, 0, 10, 0, None, None, None, 0, C.byref(n),
+                                   C.byref(tw), None))
+    assert (n.value, tw.value) == (0, 0)
+    N.check(L.bmm_split_window_dev(None, 3, 1, 0, 1, None, None, None, 0, C.byref(n),
+                                   C.byref(tw), None))
+    assert (n.value, tw.value) == (0, 0)
